@@ -1,0 +1,209 @@
+// board.cuh -- device-side board primitives for the 2048 tablebase engine.
+//
+// A board is a u64 of 16 nibbles; nibble 0 (bits 63..60) is the top-left cell,
+// cells run row-major (api/cablegen.h:9-12).  Row k (cells 4k..4k+3) occupies
+// bits 63-16k .. 48-16k, its leftmost cell in the row's high nibble.
+//
+// Geometry is expressed through three involutions that map onto cheap
+// 32-bit byte permutes: V (reverse the row order), H (reverse each row) and
+// T (transpose).  The eight symmetries of the square are {X, X.T} for
+// X in {id, V, H, VH}; the canonical board is the unsigned maximum over that
+// orbit, which equals the reference's scalar canonicalize_b
+// (src/board.c:314-337) because both take the maximum over the same set.
+//
+// Moves: the reference moves up by rotating clockwise and moving right, down
+// by rotating clockwise and moving left (src/board.c:195-214), and right uses
+// the mirrored LUT.  Since rot_cw = H.T and right(x) = H(left(H x)) (checked
+// exhaustively against the reference LUT for every settings combination), the
+// canonical results of the four directions are canon(left(y)) for the four
+// "views" y in {b, H b, T b, H T b}; only the left-move row table is needed.
+#pragma once
+#include <stdint.h>
+
+namespace cgb {
+
+typedef uint64_t u64;
+typedef unsigned int u32;
+
+__host__ __device__ __forceinline__ u64 make64(u32 hi, u32 lo) { return ((u64)hi << 32) | lo; }
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ u32 prmt(u32 a, u32 sel) { return __byte_perm(a, 0, sel); }
+#else
+inline u32 prmt(u32 a, u32 sel)
+{
+    u32 out = 0;
+    for (int i = 0; i < 4; i++) {
+        u32 s = (sel >> (4 * i)) & 7;
+        u32 byte = s < 4 ? (a >> (8 * s)) & 0xFF : 0;
+        out |= byte << (8 * i);
+    }
+    return out;
+}
+#endif
+
+// reverse the nibbles of each 16-bit half-word of a 32-bit word
+__host__ __device__ __forceinline__ u32 rev_rows32(u32 x)
+{
+    x = prmt(x, 0x2301);                                      // swap bytes inside each half-word
+    return ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4); // swap nibbles inside each byte
+}
+
+// V: reverse the order of the four rows
+__host__ __device__ __forceinline__ u64 flip_v(u64 b)
+{
+    u32 hi = (u32)(b >> 32), lo = (u32)b;
+    return make64(prmt(lo, 0x1032), prmt(hi, 0x1032));
+}
+
+// H: mirror every row left<->right
+__host__ __device__ __forceinline__ u64 flip_h(u64 b)
+{
+    return make64(rev_rows32((u32)(b >> 32)), rev_rows32((u32)b));
+}
+
+// T: transpose the 4x4 nibble matrix (cell (r,c) <-> (c,r)) by two delta swaps:
+// inside every 2x2 block, then the two off-diagonal 2x2 blocks.
+__host__ __device__ __forceinline__ u64 transpose(u64 b)
+{
+    u64 t = ((b >> 12) ^ b) & 0x0000F0F00000F0F0ull;   // cells 4,6,12,14 <-> 1,3,9,11
+    b ^= t ^ (t << 12);
+    t = ((b >> 24) ^ b) & 0x00000000FF00FF00ull;       // cells 8,9,12,13 <-> 2,3,6,7
+    b ^= t ^ (t << 24);
+    return b;
+}
+
+__host__ __device__ __forceinline__ u64 umax64(u64 a, u64 b) { return a > b ? a : b; }
+
+// canonical representative: unsigned max over the 8 symmetries
+__host__ __device__ __forceinline__ u64 canonical(u64 b)
+{
+    u64 t = transpose(b);
+    u64 bv = flip_v(b), tv = flip_v(t);
+    u64 m0 = umax64(b, bv), m1 = umax64(flip_h(b), flip_h(bv));
+    u64 m2 = umax64(t, tv), m3 = umax64(flip_h(t), flip_h(tv));
+    return umax64(umax64(m0, m1), umax64(m2, m3));
+}
+
+// reference rotate_clockwise (src/board.c:239-248): new (r,c) = old (3-c, r)
+__host__ __device__ __forceinline__ u64 rot_cw(u64 b) { return flip_h(transpose(b)); }
+__host__ __device__ __forceinline__ u64 rot_ccw(u64 b) { return transpose(flip_h(b)); }
+
+__host__ __device__ __forceinline__ int tile_at(u64 b, int cell) { return (int)((b >> (60 - 4 * cell)) & 0xF); }
+__host__ __device__ __forceinline__ u64 set_tile(u64 b, int cell, u64 v)
+{
+    const int sh = 60 - 4 * cell;
+    return (b & ~(0xFull << sh)) | (v << sh);
+}
+
+// one bit per nibble (in the nibble's low bit) for every empty cell
+__host__ __device__ __forceinline__ u64 empty_mask(u64 b)
+{
+    u64 x = b | (b >> 2);
+    x |= x >> 1;
+    return ~x & 0x1111111111111111ull;
+}
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ int popc64(u64 x) { return __popcll(x); }
+#else
+inline int popc64(u64 x) { return __builtin_popcountll(x); }
+#endif
+
+// tile sum (src/board.c:340-347): 2^e for e not in {0, 0xe, 0xf}
+__host__ __device__ __forceinline__ int tile_sum(u64 b)
+{
+    int s = 0;
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+        int e = (int)((b >> (4 * c)) & 0xF);
+        s += (e != 0 && e < 0xE) ? (1 << e) : 0;
+    }
+    return s;
+}
+
+// prune predicate (src/generate.c:98-131).  It depends only on the multiset of
+// tile values, so it may be evaluated on any orientation of the board.
+struct PruneParams {
+    long long stsl, ltc, smallest_large;
+    int enabled;
+};
+
+__host__ __device__ __forceinline__ bool prune_board(u64 b, const PruneParams &p)
+{
+    int large = 0, sl_count = 0;
+    long long small_sum = 0;
+    u32 once = 0, twice = 0;
+    bool dead = false;
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+        const int e = (int)((b >> (4 * c)) & 0xF);
+        if (e >= p.smallest_large && e < 0xE) {
+            large++;
+            if (e == p.smallest_large && sl_count < 3) {
+                sl_count++;
+            } else {
+                const u32 bit = 1u << e;
+                if (twice & bit) dead = true;
+                twice |= once & bit;
+                once |= bit;
+            }
+        } else if (e < 0xE) {
+            small_sum += 1ll << e;
+        }
+    }
+    return dead || small_sum > p.stsl + 64 || large > p.ltc;
+}
+
+// contains tile x?  (src/generate.c:89-96 returns the negation)
+__host__ __device__ __forceinline__ bool has_tile(u64 b, int x)
+{
+    if (x < 0 || x > 15) return false;
+    u64 y = b ^ (0x1111111111111111ull * (u64)x);
+    return empty_mask(y) != 0;
+}
+
+// winstate pattern test (src/solve.c:226-231): every nonzero nibble of w must match
+__host__ __device__ __forceinline__ bool matches(u64 b, u64 w)
+{
+    u64 m = w | (w >> 2);
+    m = (m | (m >> 1)) & 0x1111111111111111ull;
+    return (b & (m * 0xF)) == w;
+}
+
+// ---- the row table in shared memory -------------------------------------
+// move[row]: the row after a left move; ok bit set = the move keeps every 0xf
+// cell in place (the reference's _locked_lut, src/board.c:29-38,117).
+struct RowTable {
+    const unsigned short *move;  // 65536 entries
+    const u32 *ok;               // 2048 words, one bit per row
+};
+
+// left move of the four rows of y; returns 0 when any row is locked, else
+// sets *out and returns 1 + (changed ? 1 : 0)
+__device__ __forceinline__ int move_left(const RowTable &t, u64 y, u64 *out)
+{
+    u64 r = 0;
+    bool ok = true, changed = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const u32 row = (u32)(y >> (16 * i)) & 0xFFFFu;
+        const u32 m = t.move[row];
+        ok &= (t.ok[row >> 5] >> (row & 31)) & 1u;
+        changed |= (m != row);
+        r |= (u64)m << (16 * i);
+    }
+    *out = r;
+    return ok ? 1 + (int)changed : 0;
+}
+
+// the four move views of b: {b, H b, T b, H T b} for left, right, up, down
+__device__ __forceinline__ void views(u64 b, u64 v[4])
+{
+    v[0] = b;
+    v[1] = flip_h(b);
+    v[2] = transpose(b);
+    v[3] = flip_h(v[2]);
+}
+
+}  // namespace cgb

@@ -1,0 +1,69 @@
+// cgb_engine.h -- the engine object behind the C ABI.
+#pragma once
+#include "engine.h"
+#include "../../include/cablegen_b200.h"
+
+namespace cgb {
+
+// accumulates the device time of one phase into *acc (CUDA events)
+struct Timer {
+    cudaStream_t s;
+    double *acc;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer(cudaStream_t st, double *p) : s(st), acc(p)
+    {
+        if (acc) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, s);
+        }
+    }
+    void stop()
+    {
+        if (!acc || !a) return;
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        *acc += ms;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        a = b = nullptr;
+    }
+    ~Timer() { stop(); }
+};
+
+struct GenTimes {
+    double expand_ms = 0, sort_ms = 0, unique_ms = 0, merge_ms = 0;
+    u64 boards = 0, sorted_keys = 0, sort_passes = 0;
+};
+
+// receives each generated layer (device pointer, valid on stream s)
+struct LayerSink {
+    virtual ~LayerSink() {}
+    // set *kept = true to take ownership of the device buffer (freed later by
+    // the sink with dev_free on the engine stream)
+    virtual bool layer(int sum, u64 *d_boards, u64 n, cudaStream_t s, bool *kept) = 0;
+};
+
+struct Engine {
+    int device = -1;
+    bool ready = false;
+    cudaStream_t stream = nullptr, io_stream = nullptr;
+    DeviceRowTable rt;
+    SortWorkspace ws;
+    Counters ctr;
+    cgb_rules rules{};
+
+    static Engine &get();
+    bool init(int dev);
+    bool set_rules(const cgb_rules &r);
+    PruneParams prune_params() const;
+    bool sync();
+
+    bool move_layer(const u64 *d_in, u64 n, DevBuf<u64> &moved, GenTimes *tm);
+    bool spawn_layer(const u64 *d_moved, u64 n, DevBuf<u64> &u2, DevBuf<u64> &u4, GenTimes *tm);
+    bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm);
+};
+
+}  // namespace cgb

@@ -1,0 +1,102 @@
+// common.cuh -- shared host/device helpers of the engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+
+namespace cgb {
+
+typedef uint64_t u64;
+typedef unsigned int u32;
+
+// Device error word bits.  Every kernel that can fail ORs a bit into a
+// device-resident word that the host reads after each phase; nothing traps.
+enum : u32 {
+    ERR_LOOKBACK_TIMEOUT = 1u << 0,   // a decoupled look-back wait ran out
+    ERR_CAPACITY = 1u << 1,           // an output would exceed its buffer
+    ERR_UNSORTED = 1u << 2,           // an input that must be sorted was not
+    ERR_TOO_LARGE = 1u << 3,          // a size beyond a kernel's 32-bit counters
+};
+
+// Bounded spin: a wait on another CTA gives up after this many polls.
+constexpr u32 SPIN_LIMIT = 1u << 22;
+
+constexpr int NUM_SMS_B200 = 148;
+
+std::string err_string(u32 err);
+
+// record the first CUDA error of an API call; returns false on failure
+bool cuda_ok(cudaError_t e, const char *what, const char *file, int line);
+#define CGB_CUDA(call) ::cgb::cuda_ok((call), #call, __FILE__, __LINE__)
+
+void set_error(const std::string &msg);
+const char *last_error();
+
+#ifdef __CUDACC__
+__device__ __forceinline__ u32 ld_acquire(const u32 *p)
+{
+    u32 v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(u32 *p, u32 v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ u64 ld_acquire64(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release64(u64 *p, u64 v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ u32 lanemask_lt()
+{
+    u32 m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// inclusive warp scan
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+// exclusive block scan of one value per thread (blockDim.x a multiple of 32,
+// at most 1024); `scratch` holds 33 T.  Returns the exclusive prefix and the
+// block total in *total.  Contains __syncthreads().
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T *scratch, T *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    T inc = warp_inclusive_scan(v);
+    if (lane == 31) scratch[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < nwarps ? scratch[lane] : T(0);
+        T wi = warp_inclusive_scan(w);
+        scratch[lane] = wi - w;
+        if (lane == 31) scratch[32] = wi;
+    }
+    __syncthreads();
+    *total = scratch[32];
+    T r = scratch[warp] + inc - v;
+    __syncthreads();
+    return r;
+}
+#endif
+
+}  // namespace cgb

@@ -1,0 +1,244 @@
+// engine.cu -- device runtime: memory, the generation sweep and the solve sweep.
+//
+// Generation (src/generate.c:409-615) keeps the rolling sets on the device:
+//   S_s    boards of tile sum s still to move (the reference's n)
+//   U4     sorted unique 4-spawns of the previous layer (the reference's n4,
+//          carried to become part of n2)
+// and per layer runs
+//   moved = unique(sort(expand_moves(S_s)))           -> the layer s.boards
+//   U2    = unique(sort(spawn2(moved)))
+//   U4'   = unique(sort(spawn4(moved)))
+//   S_s+2 = merge_unique(U2, U4)                       (src/generate.c:530-544)
+// Layers go to a LayerSink: it keeps them in HBM (the resident gen+solve
+// run) or copies them out (files through the C API).
+//
+// Solve (src/solve.c:172-224) walks the layers top-down with the s+2 and s+4
+// tables resident.
+#include "engine.h"
+#include "cgb_engine.h"
+#include <algorithm>
+#include <mutex>
+
+namespace cgb {
+
+// ---- errors -----------------------------------------------------------------
+static std::string g_last_error;
+static std::mutex g_err_mu;
+
+void set_error(const std::string &msg)
+{
+    std::lock_guard<std::mutex> g(g_err_mu);
+    g_last_error = msg;
+}
+const char *last_error()
+{
+    std::lock_guard<std::mutex> g(g_err_mu);
+    return g_last_error.c_str();
+}
+bool cuda_ok(cudaError_t e, const char *what, const char *file, int line)
+{
+    if (e == cudaSuccess) return true;
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s:%d: %s failed: %s", file, line, what, cudaGetErrorString(e));
+    set_error(buf);
+    return false;
+}
+std::string err_string(u32 err)
+{
+    std::string s;
+    if (err & ERR_LOOKBACK_TIMEOUT) s += "[look-back wait timed out]";
+    if (err & ERR_CAPACITY) s += "[output capacity exceeded]";
+    if (err & ERR_UNSORTED) s += "[input not sorted]";
+    if (err & ERR_TOO_LARGE) s += "[size beyond 32-bit counters]";
+    return s.empty() ? "[none]" : s;
+}
+
+// ---- memory -----------------------------------------------------------------
+bool dev_alloc(void **p, u64 bytes, cudaStream_t s)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 256;
+    return CGB_CUDA(cudaMallocAsync(p, bytes, s));
+}
+void dev_free(void *p, cudaStream_t s)
+{
+    if (p) cudaFreeAsync(p, s);
+}
+
+// ---- engine -----------------------------------------------------------------
+Engine &Engine::get()
+{
+    static Engine e;
+    return e;
+}
+
+bool Engine::init(int dev)
+{
+    if (ready && dev == device) return true;
+    if (!CGB_CUDA(cudaSetDevice(dev))) return false;
+    device = dev;
+    if (!stream && !CGB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking))) return false;
+    if (!io_stream && !CGB_CUDA(cudaStreamCreateWithFlags(&io_stream, cudaStreamNonBlocking))) return false;
+    cudaMemPool_t pool;
+    if (!CGB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev))) return false;
+    u64 keep = ~0ull;  // keep freed blocks cached in the pool between layers
+    if (!CGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep))) return false;
+    if (!ctr.d) {
+        void *p;
+        if (!CGB_CUDA(cudaMalloc(&p, 64 * sizeof(u64)))) return false;
+        ctr.d = (u64 *)p;
+        ctr.err = (u32 *)(ctr.d + 32);
+        if (!CGB_CUDA(cudaMemset(p, 0, 64 * sizeof(u64)))) return false;
+    }
+    ready = true;
+    return true;
+}
+
+bool Engine::set_rules(const cgb_rules &r)
+{
+    rules = r;
+    return upload_row_table(rt, r.free_formation ? 1 : 0, r.ignore_f ? 1 : 0, stream);
+}
+
+PruneParams Engine::prune_params() const
+{
+    PruneParams p;
+    p.enabled = rules.prune ? 1 : 0;
+    p.stsl = rules.stsl;
+    p.ltc = rules.ltc;
+    p.smallest_large = rules.smallest_large;
+    return p;
+}
+
+bool Engine::sync() { return CGB_CUDA(cudaStreamSynchronize(stream)); }
+
+// moved = unique(sort(expand_moves(S)))
+bool Engine::move_layer(const u64 *d_in, u64 n, DevBuf<u64> &moved, GenTimes *tm)
+{
+    cudaStream_t s = stream;
+    DevBuf<u64> a, b;
+    const u64 cap = 4 * n;
+    if (!grow(a, cap, s) || !grow(b, cap, s)) return false;
+    u64 nr = 0;
+    {
+        Timer t(s, tm ? &tm->expand_ms : nullptr);
+        if (!expand_moves(d_in, n, a.p, cap, &nr, rt, prune_params(), ctr, s)) return false;
+    }
+    u64 *sorted = a.p;
+    SortStats st;
+    {
+        Timer t(s, tm ? &tm->sort_ms : nullptr);
+        if (!sort_keys(a.p, b.p, nr, &sorted, ws, s, &st)) return false;
+    }
+    if (tm) {
+        tm->sorted_keys += nr;
+        tm->sort_passes += (u64)st.passes * nr;
+    }
+    // unique from the sorted buffer into the other one
+    DevBuf<u64> src = (sorted == a.p) ? a : b;
+    DevBuf<u64> dst = (sorted == a.p) ? b : a;
+    u64 nm = 0;
+    {
+        Timer t(s, tm ? &tm->unique_ms : nullptr);
+        if (!unique_keys(src.p, nr, dst.p, &nm, ws, s)) return false;
+    }
+    drop(src, s);
+    drop(moved, s);
+    moved = dst;
+    moved.n = nm;
+    return true;
+}
+
+// U2 / U4: sorted unique canonical 2-spawns and 4-spawns of the moved layer
+bool Engine::spawn_layer(const u64 *d_moved, u64 n, DevBuf<u64> &u2, DevBuf<u64> &u4, GenTimes *tm)
+{
+    cudaStream_t s = stream;
+    u64 total = 0;
+    if (!count_spawns(d_moved, n, &total, ctr, s)) return false;
+    DevBuf<u64> x2, x4, spare;
+    if (!grow(x2, total, s) || !grow(x4, total, s) || !grow(spare, total, s)) return false;
+    u64 ns = 0;
+    {
+        Timer t(s, tm ? &tm->expand_ms : nullptr);
+        if (!expand_spawns(d_moved, n, x2.p, x4.p, total, &ns, ctr, s)) return false;
+    }
+    DevBuf<u64> *outs[2] = {&u2, &u4};
+    DevBuf<u64> ins[2] = {x2, x4};
+    for (int k = 0; k < 2; k++) {
+        DevBuf<u64> in = ins[k];
+        u64 *sorted = in.p;
+        SortStats st;
+        {
+            Timer t(s, tm ? &tm->sort_ms : nullptr);
+            if (!sort_keys(in.p, spare.p, ns, &sorted, ws, s, &st)) return false;
+        }
+        if (tm) {
+            tm->sorted_keys += ns;
+            tm->sort_passes += (u64)st.passes * ns;
+        }
+        DevBuf<u64> full = (sorted == in.p) ? in : spare;   // holds the sorted keys
+        DevBuf<u64> free_ = (sorted == in.p) ? spare : in;  // receives the unique keys
+        u64 nu = 0;
+        {
+            Timer t(s, tm ? &tm->unique_ms : nullptr);
+            if (!unique_keys(full.p, ns, free_.p, &nu, ws, s)) return false;
+        }
+        drop(*outs[k], s);
+        *outs[k] = free_;
+        outs[k]->n = nu;
+        spare = full;  // its contents are no longer needed
+    }
+    drop(spare, s);
+    return true;
+}
+
+bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm)
+{
+    cudaStream_t s = stream;
+    DevBuf<u64> S, U4, moved, U2, next;
+    if (!grow(S, n_init, s)) return false;
+    if (n_init && !CGB_CUDA(cudaMemcpyAsync(S.p, h_initial, n_init * 8, cudaMemcpyHostToDevice, s))) return false;
+    S.n = n_init;
+    bool ok = true;
+    for (int layer = start; layer <= end && ok; layer += 2) {
+        ok = move_layer(S.p, S.n, moved, tm);
+        if (!ok) break;
+        drop(S, s);
+        ok = spawn_layer(moved.p, moved.n, U2, next, tm);
+        if (!ok) break;
+        // S_{s+2} = U2 u U4(previous layer)
+        if (!grow(S, U2.n + U4.n, s)) {
+            ok = false;
+            break;
+        }
+        u64 nm = 0;
+        {
+            Timer t(s, tm ? &tm->merge_ms : nullptr);
+            ok = merge_unique(U2.p, U2.n, U4.p, U4.n, S.p, &nm, ws, s);
+        }
+        if (!ok) break;
+        S.n = nm;
+        drop(U2, s);
+        drop(U4, s);
+        U4 = next;
+        next.p = nullptr;
+        next.cap = next.n = 0;
+        if (tm) tm->boards += moved.n;
+        // hand the layer to the sink (it may keep the buffer)
+        bool kept = false;
+        ok = sink.layer(layer, moved.p, moved.n, s, &kept);
+        if (kept) {
+            moved.p = nullptr;
+            moved.cap = moved.n = 0;
+        }
+    }
+    drop(S, s);
+    drop(U4, s);
+    drop(U2, s);
+    drop(moved, s);
+    drop(next, s);
+    if (ok) ok = sync();
+    return ok;
+}
+
+}  // namespace cgb

@@ -1,0 +1,120 @@
+// engine.h -- internal interfaces of the CUDA engine (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "board.cuh"
+
+namespace cgb {
+
+// ---- sort / unique / merge (sort.cu) ------------------------------------
+struct SortWorkspace {
+    static constexpr int SMALL_WORDS = 4096;
+    u32 *small = nullptr;       // histograms, tile counters, error word, counts
+    u32 *lookback = nullptr;    // decoupled look-back state
+    u64 lookback_bytes = 0;
+    bool reserve(u64 n, cudaStream_t s);
+    void release(cudaStream_t s);
+};
+
+struct SortStats {
+    int passes = 0;
+    u64 n = 0;
+};
+
+int sort_plan(const u32 *hist_host, u64 n, int *digits);
+// sorts keys[0,n) ascending using tmp[0,n); *sorted points at keys or tmp
+bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cudaStream_t s,
+               SortStats *stats = nullptr);
+// out must not alias in
+bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s);
+// sorted union of two sorted duplicate-free runs, without repeats
+bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_out, SortWorkspace &ws,
+                  cudaStream_t s);
+
+// ---- row table and expansion (expand.cu) ---------------------------------
+struct DeviceRowTable {
+    unsigned short *move = nullptr;  // 65536 rows, left move
+    u32 *ok = nullptr;               // 2048 words: bit set = the move keeps 0xf cells
+    int free_formation = -1, ignore_f = -1;
+};
+
+// the left-move row table of the reference (src/board.c:62-132), host side
+void build_row_table(int free_formation, int ignore_f, unsigned short *move, u32 *ok);
+bool upload_row_table(DeviceRowTable &t, int free_formation, int ignore_f, cudaStream_t s);
+
+struct Counters {
+    u64 *d = nullptr;   // device words: [0] output count, [1] spawn total, [2..] scratch
+    u32 *err = nullptr; // device error word
+};
+
+// move + prune + canonicalise every board; out needs room for 4n boards
+bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
+                  const PruneParams &p, Counters &c, cudaStream_t s);
+// number of empty cells over all boards (exact size of the spawn streams)
+bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s);
+// canonical 2-spawn and 4-spawn of every empty cell of every board
+bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c,
+                   cudaStream_t s);
+
+// ---- solve (solve.cu) ------------------------------------------------------
+struct SolveRules {
+    int nox = 0;       // char semantics already applied
+    int score = 0;
+    const u64 *winstates = nullptr;  // device, expanded x8
+    int n_winstates = 0;
+};
+
+// lookup index over one solved layer: bucket offsets over the key bits that
+// follow the layer's common prefix
+struct LayerIndex {
+    const u64 *keys = nullptr;
+    const void *vals = nullptr;   // double or float, aligned with keys
+    u64 n = 0;
+    const u32 *bucket = nullptr;  // 2^bits + 1 offsets (null: plain bisection)
+    int shift = 0;                // bucket = (key << prefix) >> (64 - bits)
+    int prefix = 0;
+    int bits = 0;
+    u64 prefix_value = 0;         // the shared high bits (key >> (64 - prefix))
+};
+
+bool build_index(LayerIndex &ix, u32 **bucket_storage, u64 *bucket_capacity, int bits_hint, cudaStream_t s);
+
+bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s);
+bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, const LayerIndex &t4,
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s);
+
+// ---- device memory --------------------------------------------------------
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    u64 n = 0;     // elements in use
+    u64 cap = 0;   // elements allocated
+};
+
+bool dev_alloc(void **p, u64 bytes, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
+template <typename T>
+bool grow(DevBuf<T> &b, u64 n, cudaStream_t s)
+{
+    if (b.cap >= n && b.p) return true;
+    if (b.p) dev_free(b.p, s);
+    b.p = nullptr;
+    b.cap = 0;
+    u64 want = n < 64 ? 64 : n;
+    if (!dev_alloc((void **)&b.p, want * sizeof(T), s)) return false;
+    b.cap = want;
+    return true;
+}
+template <typename T>
+void drop(DevBuf<T> &b, cudaStream_t s)
+{
+    if (b.p) dev_free(b.p, s);
+    b.p = nullptr;
+    b.n = b.cap = 0;
+}
+
+}  // namespace cgb

@@ -1,0 +1,257 @@
+// expand.cu -- the per-board work of one generation layer.
+//
+// expand_moves restates the move workers of the reference
+// (src/generate.c:133-175, OpenCL move_kernel src/cl/generate.cl:249-282):
+// optional prune of the input, the four moves, prune of each moved board,
+// canonicalisation.  The left-move row table (128 KiB of u16 + an 8 KiB
+// "keeps 0xf in place" bitset) is staged into shared memory once per CTA of a
+// persistent grid; right/up/down reuse it through the board views of
+// board.cuh.  Results are appended with one atomic per CTA iteration after a
+// block scan, so the output is compact (no 4N slot array + separate scan).
+//
+// expand_spawns restates src/generate.c:177-199: every empty cell receives a
+// 2 (nibble 1) and a 4 (nibble 2); both boards are canonicalised.  The exact
+// output size is counted first (no slot cap, unlike SPAWN_SLOTS=4 of the
+// OpenCL path, src/cl/generate.cl:215-245).
+#include "engine.h"
+
+namespace cgb {
+
+constexpr int EXP_THREADS = 512;
+constexpr int TABLE_BYTES = 65536 * 2 + 2048 * 4;
+
+void build_row_table(int free_formation, int ignore_f, unsigned short *move, u32 *ok)
+{
+    // One row = four cells, travel toward cell 0.  Restates move()
+    // (src/board.c:62-98): slide the non-empty cells forward, merge equal
+    // neighbours below 0xE once each from the front, slide again.  With
+    // ignore_f, 0xF cells at the far end are walls.  A row is locked when a
+    // cell that held 0xF no longer does (src/board.c:29-38), unless the
+    // formation is free.
+    for (u32 row = 0; row < 65536; row++) {
+        int t[4], pre[4];
+        for (int c = 0; c < 4; c++) pre[c] = t[c] = (row >> (12 - 4 * c)) & 0xF;
+        int n = 4;
+        if (ignore_f)
+            while (n > 0 && t[n - 1] == 0xF) n--;
+        auto slide = [&]() {
+            int w = 0, tmp[4] = {0, 0, 0, 0};
+            for (int i = 0; i < n; i++)
+                if (t[i]) tmp[w++] = t[i];
+            for (int i = 0; i < n; i++) t[i] = tmp[i];
+        };
+        slide();
+        for (int i = 0; i + 1 < n; i++) {
+            if (t[i] && t[i] == t[i + 1] && t[i] < 0xE) {
+                for (int j = i + 1; j + 1 < n; j++) t[j] = t[j + 1];
+                t[n - 1] = 0;
+                t[i] += 1;
+            }
+        }
+        slide();
+        u32 out = (u32)((t[0] << 12) | (t[1] << 8) | (t[2] << 4) | t[3]);
+        bool vacated = false;
+        if (!free_formation)
+            for (int c = 0; c < 4; c++)
+                if (pre[c] == 0xF && t[c] != 0xF) vacated = true;
+        move[row] = (unsigned short)out;
+        if (row % 32 == 0) ok[row / 32] = 0;
+        if (!vacated) ok[row / 32] |= 1u << (row % 32);
+    }
+    move[0] = 0;          // src/board.c:126-129
+    move[0xFFFF] = 0xFFFF;
+}
+
+bool upload_row_table(DeviceRowTable &t, int free_formation, int ignore_f, cudaStream_t s)
+{
+    if (t.move && t.free_formation == free_formation && t.ignore_f == ignore_f) return true;
+    std::vector<unsigned short> mv(65536);
+    std::vector<u32> ok(2048);
+    build_row_table(free_formation, ignore_f, mv.data(), ok.data());
+    if (!t.move) {
+        void *p = nullptr;
+        if (!CGB_CUDA(cudaMalloc(&p, TABLE_BYTES))) return false;
+        t.move = (unsigned short *)p;
+        t.ok = (u32 *)((char *)p + 65536 * 2);
+    }
+    if (!CGB_CUDA(cudaMemcpyAsync(t.move, mv.data(), 65536 * 2, cudaMemcpyHostToDevice, s))) return false;
+    if (!CGB_CUDA(cudaMemcpyAsync(t.ok, ok.data(), 2048 * 4, cudaMemcpyHostToDevice, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    t.free_formation = free_formation;
+    t.ignore_f = ignore_f;
+    return true;
+}
+
+__device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned short *g_move, const u32 *g_ok)
+{
+    const uint4 *src = (const uint4 *)g_move;
+    uint4 *dst = (uint4 *)smem;
+    for (int i = threadIdx.x; i < TABLE_BYTES / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
+                                                                      u64 *__restrict__ out, u64 cap,
+                                                                      u64 *out_count, const unsigned short *g_move,
+                                                                      const u32 *g_ok, PruneParams pp, u32 *err)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u64 base_sh;
+    stage_table(smem, g_move, g_ok);
+    const RowTable t{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    const u64 stride = (u64)gridDim.x * EXP_THREADS;
+    for (u64 first = (u64)blockIdx.x * EXP_THREADS; first < n; first += stride) {
+        const u64 idx = first + threadIdx.x;
+        u64 r[4] = {0, 0, 0, 0};
+        u32 mask = 0;
+        if (idx < n) {
+            const u64 b = in[idx];
+            if (!(pp.enabled && prune_board(b, pp))) {
+                u64 v[4];
+                views(b, v);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    u64 m;
+                    if (move_left(t, v[k], &m) == 2 && !(pp.enabled && prune_board(m, pp))) {
+                        r[k] = canonical(m);
+                        mask |= 1u << k;
+                    }
+                }
+            }
+        }
+        const u32 cnt = __popc(mask);
+        u32 total;
+        const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
+        if (threadIdx.x == 0) base_sh = total ? (u64)atomicAdd((unsigned long long *)out_count, (unsigned long long)total) : 0;
+        __syncthreads();
+        u64 pos = base_sh + excl;
+        if (pos + cnt > cap) {
+            if (cnt) atomicOr(err, ERR_CAPACITY);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (mask & (1u << k)) out[pos++] = r[k];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) count_spawns_kernel(const u64 *__restrict__ in, u64 n, u64 *total)
+{
+    __shared__ u32 scratch[33];
+    u64 acc = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        acc += popc64(empty_mask(in[i]));
+    u32 tot;
+    block_exclusive_scan<u32>((u32)acc, scratch, &tot);
+    if (threadIdx.x == 0 && tot) atomicAdd((unsigned long long *)total, (unsigned long long)tot);
+}
+
+__global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restrict__ in, u64 n,
+                                                            u64 *__restrict__ out2, u64 *__restrict__ out4,
+                                                            u64 cap, u64 *out_count, u32 *err)
+{
+    __shared__ u32 scan_scratch[33];
+    __shared__ u64 base_sh;
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 first = (u64)blockIdx.x * blockDim.x; first < n; first += stride) {
+        const u64 idx = first + threadIdx.x;
+        const u64 b = idx < n ? in[idx] : ~0ull;
+        u64 e = idx < n ? empty_mask(b) : 0;
+        const u32 cnt = popc64(e);
+        u32 total;
+        const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
+        if (threadIdx.x == 0) base_sh = total ? (u64)atomicAdd((unsigned long long *)out_count, (unsigned long long)total) : 0;
+        __syncthreads();
+        u64 pos = base_sh + excl;
+        if (pos + cnt > cap) {
+            if (cnt) atomicOr(err, ERR_CAPACITY);
+        } else {
+            while (e) {
+                const int bit = 63 - __clzll(e);  // nibble's low bit
+                e &= ~(1ull << bit);
+                out2[pos] = canonical(b | (1ull << bit));
+                out4[pos] = canonical(b | (2ull << bit));
+                pos++;
+            }
+        }
+    }
+}
+
+static int sm_count()
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = NUM_SMS_B200;
+    }
+    return sms;
+}
+
+static bool read_word(u64 *dst, const u64 *src, cudaStream_t s)
+{
+    if (!CGB_CUDA(cudaMemcpyAsync(dst, src, sizeof(u64), cudaMemcpyDeviceToHost, s))) return false;
+    return CGB_CUDA(cudaStreamSynchronize(s));
+}
+
+static bool check(Counters &c, cudaStream_t s, const char *what)
+{
+    u32 e = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(&e, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    if (e) {
+        set_error(std::string(what) + ": device error " + err_string(e));
+        return false;
+    }
+    return true;
+}
+
+bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
+                  const PruneParams &p, Counters &c, cudaStream_t s)
+{
+    *n_out = 0;
+    if (n == 0) return true;
+    static bool attr = false;
+    if (!attr) {
+        if (!CGB_CUDA(cudaFuncSetAttribute(expand_moves_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           TABLE_BYTES)))
+            return false;
+        attr = true;
+    }
+    if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+    const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
+    const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
+    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    if (!read_word(n_out, c.d, s)) return false;
+    return check(c, s, "expand_moves");
+}
+
+bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s)
+{
+    *total = 0;
+    if (n == 0) return true;
+    if (!CGB_CUDA(cudaMemsetAsync(c.d + 1, 0, sizeof(u64), s))) return false;
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
+    count_spawns_kernel<<<grid, 256, 0, s>>>(in, n, c.d + 1);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    return read_word(total, c.d + 1, s);
+}
+
+bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c, cudaStream_t s)
+{
+    *n_out = 0;
+    if (n == 0) return true;
+    if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
+    expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    if (!read_word(n_out, c.d, s)) return false;
+    return check(c, s, "expand_spawns");
+}
+
+}  // namespace cgb

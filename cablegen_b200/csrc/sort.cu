@@ -1,0 +1,524 @@
+// sort.cu -- device-wide u64 sort, unique and merge for board sets.
+//
+// Replaces the reference's per-thread fluxsort + serial k-way merge
+// (src/array.c:246-291, inc/external/fluxsort.h:112-120): layers must come out
+// ascending and duplicate-free, bit-for-bit.
+//
+// * LSD radix sort with 8-bit digits in the single-pass "onesweep" form
+//   (Adinets & Merrill 2022): one histogram pass for all eight digits, then
+//   one pass per non-constant digit that ranks a 4096-key tile in shared
+//   memory and finds its global bin offsets by a decoupled look-back.  Digits
+//   on which every key agrees (the 0xff prefix that canonical formation
+//   boards share) are skipped.
+// * unique: adjacent-difference flags, ballot/popc compaction, decoupled
+//   look-back for the tile prefix.
+// * merge_unique: merge-path partition of two sorted unique runs, per-thread
+//   sequential merge in shared memory, the same compaction.
+//
+// Every look-back wait is bounded (SPIN_LIMIT polls); on timeout the kernel
+// sets ERR_LOOKBACK_TIMEOUT in the error word and finishes without waiting.
+#include "common.cuh"
+#include "engine.h"
+
+namespace cgb {
+
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_KPT = 16;
+constexpr int SORT_TILE = SORT_THREADS * SORT_KPT;  // 4096 keys per tile
+constexpr int RADIX = 256;
+constexpr u32 LB_AGG = 1u << 30, LB_PRE = 2u << 30, LB_MASK = (1u << 30) - 1;
+
+constexpr int UNQ_THREADS = 256;
+constexpr int UNQ_KPT = 16;
+constexpr int UNQ_TILE = UNQ_THREADS * UNQ_KPT;
+
+constexpr int MRG_THREADS = 256;
+constexpr int MRG_KPT = 8;
+constexpr int MRG_TILE = MRG_THREADS * MRG_KPT;
+
+// ---------------------------------------------------------------------------
+// histogram of all eight byte digits in one pass
+__global__ void __launch_bounds__(256) digit_histogram_kernel(const u64 *__restrict__ keys, u64 n,
+                                                              u32 *__restrict__ hist)
+{
+    __shared__ u32 sh[2][8 * RADIX];  // two copies halve same-bin contention
+    for (int i = threadIdx.x; i < 2 * 8 * RADIX; i += blockDim.x) (&sh[0][0])[i] = 0;
+    __syncthreads();
+    u32 *mine = sh[(threadIdx.x >> 5) & 1];
+    const int lane = threadIdx.x & 31;
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 base = (u64)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const u64 i = base + threadIdx.x;
+        const bool ok = i < n;
+        const u64 k = ok ? keys[i] : 0;
+        const u32 act = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+        for (int d = 0; d < 8; d++) {
+            const u32 dig = (u32)(k >> (8 * d)) & 0xFF;
+            // a warp whose keys all share this digit adds once
+            const u32 first = __shfl_sync(0xffffffffu, dig, 0);
+            const bool uniform = __all_sync(0xffffffffu, !ok || dig == first) && act == 0xffffffffu;
+            if (uniform) {
+                if (lane == 0) atomicAdd(&mine[d * RADIX + dig], 32u);
+            } else if (ok) {
+                atomicAdd(&mine[d * RADIX + dig], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * RADIX; i += blockDim.x) {
+        const u32 v = sh[0][i] + sh[1][i];
+        if (v) atomicAdd(&hist[i], v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// one digit pass: src -> dst, stable by the digit at `shift`
+__global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst,
+                                                                u32 n, int shift, const u32 *__restrict__ digit_hist,
+                                                                u32 *lookback, u32 *tile_counter, u32 *err)
+{
+    __shared__ u64 keys_sh[SORT_TILE];
+    __shared__ u32 warp_hist[SORT_THREADS / 32][RADIX];
+    __shared__ u32 bin_local[RADIX];
+    __shared__ u32 bin_global[RADIX];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u32 tile_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < (SORT_THREADS / 32) * RADIX; i += SORT_THREADS) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const u32 tile = tile_sh;
+    const u32 tile_base = tile * SORT_TILE;
+    const u32 warp_base = tile_base + warp * (SORT_KPT * 32);
+
+    u64 k[SORT_KPT];
+    u32 rank[SORT_KPT];
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        k[i] = idx < n ? src[idx] : 0;
+    }
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        const bool ok = idx < n;
+        const u32 d = ok ? (u32)(k[i] >> shift) & 0xFF : 0x100u;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        u32 base = 0;
+        if (ok && lane == leader) {
+            base = warp_hist[warp][d];
+            warp_hist[warp][d] = base + __popc(peers);
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        rank[i] = base + __popc(peers & lt);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // per bin: warp offsets inside the tile, tile count, look-back
+    const u32 d = threadIdx.x;  // SORT_THREADS == RADIX
+    u32 cnt = 0;
+#pragma unroll
+    for (int w = 0; w < SORT_THREADS / 32; w++) {
+        const u32 c = warp_hist[w][d];
+        warp_hist[w][d] = cnt;
+        cnt += c;
+    }
+    u32 *lb = lookback + (u64)tile * RADIX + d;
+    u32 excl = 0;
+    if (tile == 0) {
+        st_release(lb, LB_PRE | cnt);
+    } else {
+        st_release(lb, LB_AGG | cnt);
+        int j = (int)tile - 1;
+        u32 spins = 0;
+        while (j >= 0) {
+            const u32 v = ld_acquire(lookback + (u64)j * RADIX + d);
+            const u32 flag = v & ~LB_MASK;
+            if (flag == 0) {
+                if (++spins > SPIN_LIMIT) {
+                    atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                    break;
+                }
+                continue;
+            }
+            excl += v & LB_MASK;
+            if (flag == LB_PRE) break;
+            j--;
+        }
+        st_release(lb, LB_PRE | (excl + cnt));
+    }
+    u32 total;
+    const u32 gexcl = block_exclusive_scan<u32>(digit_hist[d], scan_scratch, &total);
+    const u32 lstart = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
+    bin_local[d] = lstart;
+    bin_global[d] = gexcl + excl;
+    __syncthreads();
+
+#pragma unroll
+    for (int i = 0; i < SORT_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        if (idx < n) {
+            const u32 dd = (u32)(k[i] >> shift) & 0xFF;
+            keys_sh[bin_local[dd] + warp_hist[warp][dd] + rank[i]] = k[i];
+        }
+    }
+    __syncthreads();
+    const u32 tile_n = min((u32)SORT_TILE, n - tile_base);
+    for (u32 j = threadIdx.x; j < tile_n; j += SORT_THREADS) {
+        const u64 key = keys_sh[j];
+        const u32 dd = (u32)(key >> shift) & 0xFF;
+        const u32 g = bin_global[dd] + (j - bin_local[dd]);
+        if (g < n) dst[g] = key;
+        else atomicOr(err, ERR_CAPACITY);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// decoupled look-back over one u32 count per tile; returns the exclusive prefix
+__device__ __forceinline__ u32 tile_lookback(u32 *lookback, u32 tile, u32 count, u32 *err)
+{
+    u32 excl = 0;
+    if (tile == 0) {
+        st_release(lookback, LB_PRE | count);
+        return 0;
+    }
+    st_release(lookback + tile, LB_AGG | count);
+    int j = (int)tile - 1;
+    u32 spins = 0;
+    while (j >= 0) {
+        const u32 v = ld_acquire(lookback + j);
+        const u32 flag = v & ~LB_MASK;
+        if (flag == 0) {
+            if (++spins > SPIN_LIMIT) {
+                atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            continue;
+        }
+        excl += v & LB_MASK;
+        if (flag == LB_PRE) break;
+        j--;
+    }
+    st_release(lookback + tile, LB_PRE | (excl + count));
+    return excl;
+}
+
+// padded shared-memory index for blocked reads of 16 consecutive u64
+__device__ __forceinline__ u32 pad16(u32 j) { return j + (j >> 4); }
+
+// unique: in (sorted) -> out, dropping repeats; *out_count = number kept
+__global__ void __launch_bounds__(UNQ_THREADS) unique_kernel(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out,
+                                                             u32 *lookback, u32 *tile_counter, u32 *out_count,
+                                                             u32 *err)
+{
+    __shared__ u64 keys_sh[UNQ_TILE + UNQ_TILE / 16];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u32 tile_sh, prefix_sh;
+    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const u32 tile = tile_sh;
+    const u32 tile_base = tile * UNQ_TILE;
+    const u32 tile_n = min((u32)UNQ_TILE, n - tile_base);
+    for (u32 j = threadIdx.x; j < tile_n; j += UNQ_THREADS) keys_sh[pad16(j)] = in[tile_base + j];
+    __syncthreads();
+    const u64 before = tile_base ? in[tile_base - 1] : 0;
+    // thread t owns keys [16t, 16t+16) of the tile
+    u32 flags = 0;
+    u64 prev = (threadIdx.x == 0) ? before : 0;
+    if (threadIdx.x > 0 && 16 * threadIdx.x <= tile_n) prev = keys_sh[pad16(16 * threadIdx.x - 1)];
+#pragma unroll
+    for (int i = 0; i < UNQ_KPT; i++) {
+        const u32 j = 16 * threadIdx.x + i;
+        if (j < tile_n) {
+            const u64 v = keys_sh[pad16(j)];
+            const bool first = (tile_base + j == 0) || v != prev;
+            if (first) flags |= 1u << i;
+            if (tile_base + j > 0 && v < prev) atomicOr(err, ERR_UNSORTED);
+            prev = v;
+        }
+    }
+    const u32 cnt = __popc(flags);
+    u32 tile_total;
+    const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &tile_total);
+    // gather the kept keys in place (kept rank <= position, threads ordered)
+    u64 kept[UNQ_KPT];
+#pragma unroll
+    for (int i = 0; i < UNQ_KPT; i++) kept[i] = keys_sh[pad16(16 * threadIdx.x + i)];
+    __syncthreads();
+    u32 w = excl;
+#pragma unroll
+    for (int i = 0; i < UNQ_KPT; i++)
+        if (flags & (1u << i)) keys_sh[pad16(w++)] = kept[i];
+    if (threadIdx.x == 0) prefix_sh = tile_lookback(lookback, tile, tile_total, err);
+    __syncthreads();
+    const u32 prefix = prefix_sh;
+    for (u32 j = threadIdx.x; j < tile_total; j += UNQ_THREADS) {
+        if (prefix + j < n) out[prefix + j] = keys_sh[pad16(j)];
+        else atomicOr(err, ERR_CAPACITY);
+    }
+    if (threadIdx.x == 0 && tile_base + UNQ_TILE >= n) *out_count = prefix + tile_total;
+}
+
+// ---------------------------------------------------------------------------
+// merge path: for output diagonal `diag`, number of elements taken from a
+// (ties go to a first)
+__device__ __forceinline__ u32 merge_path(const u64 *a, u32 na, const u64 *b, u32 nb, u32 diag)
+{
+    u32 lo = diag > nb ? diag - nb : 0;
+    u32 hi = diag < na ? diag : na;
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void merge_partition_kernel(const u64 *__restrict__ a, u32 na, const u64 *__restrict__ b, u32 nb,
+                                       u32 *splits, u32 ntiles)
+{
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > ntiles) return;
+    const u32 diag = min((u64)t * MRG_TILE, (u64)na + nb);
+    splits[t] = merge_path(a, na, b, nb, diag);
+}
+
+__global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__restrict__ a, u32 na,
+                                                                   const u64 *__restrict__ b, u32 nb,
+                                                                   const u32 *__restrict__ splits,
+                                                                   u64 *__restrict__ out, u32 *lookback,
+                                                                   u32 *tile_counter, u32 *out_count, u32 *err)
+{
+    __shared__ u64 in_sh[MRG_TILE];
+    __shared__ u64 out_sh[MRG_TILE + MRG_TILE / 8];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u64 last_sh[MRG_THREADS];
+    __shared__ u32 tile_sh, prefix_sh;
+    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const u32 tile = tile_sh;
+    const u64 total = (u64)na + nb;
+    const u32 d0 = (u32)min((u64)tile * MRG_TILE, total);
+    const u32 d1 = (u32)min((u64)(tile + 1) * MRG_TILE, total);
+    const u32 a0 = splits[tile], a1 = splits[tile + 1];
+    const u32 b0 = d0 - a0, b1 = d1 - a1;
+    const u32 la = a1 - a0, lb = b1 - b0;
+    for (u32 j = threadIdx.x; j < la; j += MRG_THREADS) in_sh[j] = a[a0 + j];
+    for (u32 j = threadIdx.x; j < lb; j += MRG_THREADS) in_sh[la + j] = b[b0 + j];
+    __syncthreads();
+    const u64 *sa = in_sh, *sb = in_sh + la;
+    // the merged element just before this tile
+    bool have_before = d0 > 0;
+    u64 before = 0;
+    if (have_before) {
+        if (a0 == 0) before = b[b0 - 1];
+        else if (b0 == 0) before = a[a0 - 1];
+        else before = max(a[a0 - 1], b[b0 - 1]);
+    }
+    const u32 len = d1 - d0;
+    const u32 t0 = min((u32)(threadIdx.x * MRG_KPT), len);
+    const u32 t1 = min(t0 + MRG_KPT, len);
+    u32 ia = merge_path(sa, la, sb, lb, t0);
+    u32 ib = t0 - ia;
+    u64 v[MRG_KPT];
+#pragma unroll
+    for (int i = 0; i < MRG_KPT; i++) {
+        if (t0 + i < t1) {
+            bool take_a = ib >= lb || (ia < la && sa[ia] <= sb[ib]);
+            v[i] = take_a ? sa[ia++] : sb[ib++];
+        }
+    }
+    // predecessor of this thread's first element
+    u64 mylast = 0;
+#pragma unroll
+    for (int i = 0; i < MRG_KPT; i++)
+        if (t0 + i < t1) mylast = v[i];
+    last_sh[threadIdx.x] = mylast;
+    __syncthreads();
+    u64 prev;
+    bool have_prev;
+    if (threadIdx.x == 0) {
+        prev = before;
+        have_prev = have_before;
+    } else {
+        // the previous thread always owns MRG_KPT elements when this one owns any
+        prev = last_sh[threadIdx.x - 1];
+        have_prev = true;
+    }
+    u32 flags = 0;
+#pragma unroll
+    for (int i = 0; i < MRG_KPT; i++) {
+        if (t0 + i < t1) {
+            if (!have_prev || v[i] != prev) flags |= 1u << i;
+            prev = v[i];
+            have_prev = true;
+        }
+    }
+    const u32 cnt = __popc(flags);
+    u32 tile_total;
+    const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &tile_total);
+    u32 w = excl;
+#pragma unroll
+    for (int i = 0; i < MRG_KPT; i++)
+        if (flags & (1u << i)) {
+            out_sh[w + (w >> 3)] = v[i];
+            w++;
+        }
+    if (threadIdx.x == 0) prefix_sh = tile_lookback(lookback, tile, tile_total, err);
+    __syncthreads();
+    const u32 prefix = prefix_sh;
+    for (u32 j = threadIdx.x; j < tile_total; j += MRG_THREADS) {
+        if ((u64)prefix + j < total) out[prefix + j] = out_sh[j + (j >> 3)];
+        else atomicOr(err, ERR_CAPACITY);
+    }
+    if (threadIdx.x == 0 && (u64)(tile + 1) * MRG_TILE >= total) *out_count = prefix + tile_total;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+static inline u32 ceil_div(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
+
+bool SortWorkspace::reserve(u64 n, cudaStream_t s)
+{
+    const u64 tiles = (n + MRG_TILE - 1) / MRG_TILE + 2;  // the smallest tile size bounds all
+    const u64 need = tiles * RADIX * sizeof(u32);
+    if (need <= lookback_bytes && small) return true;
+    if (lookback) cudaFreeAsync(lookback, s);
+    lookback = nullptr;
+    if (!small) {
+        if (!CGB_CUDA(cudaMallocAsync((void **)&small, SMALL_WORDS * sizeof(u32), s))) return false;
+    }
+    if (!CGB_CUDA(cudaMallocAsync((void **)&lookback, need, s))) return false;
+    lookback_bytes = need;
+    return true;
+}
+
+void SortWorkspace::release(cudaStream_t s)
+{
+    if (lookback) cudaFreeAsync(lookback, s);
+    if (small) cudaFreeAsync(small, s);
+    lookback = nullptr;
+    small = nullptr;
+    lookback_bytes = 0;
+}
+
+// small words: [0,2048) histograms, [2048,2064) tile counters, 2064 err, 2065 count
+static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065;
+
+static bool check_err(SortWorkspace &ws, cudaStream_t s, const char *what)
+{
+    u32 e = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(&e, ws.small + W_ERR, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    if (e) {
+        set_error(std::string(what) + ": device error " + err_string(e));
+        return false;
+    }
+    return true;
+}
+
+int sort_plan(const u32 *hist_host, u64 n, int *digits)
+{
+    int np = 0;
+    for (int d = 0; d < 8; d++) {
+        bool constant = false;
+        for (int b = 0; b < RADIX; b++)
+            if (hist_host[d * RADIX + b] == n) constant = true;
+        if (!constant) digits[np++] = d;
+    }
+    return np;
+}
+
+bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cudaStream_t s, SortStats *stats)
+{
+    *sorted = keys;
+    if (stats) *stats = SortStats{};
+    if (n <= 1) return true;
+    if (n > (u64)LB_MASK) {
+        set_error("sort_keys: more than 2^30 keys in one call");
+        return false;
+    }
+    if (!ws.reserve(n, s)) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (W_COUNT + 1) * sizeof(u32), s))) return false;
+    const int hist_blocks = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
+    digit_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, n, ws.small + W_HIST);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    u32 hist[8 * RADIX];
+    if (!CGB_CUDA(cudaMemcpyAsync(hist, ws.small + W_HIST, sizeof(hist), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    int digits[8];
+    const int np = sort_plan(hist, n, digits);
+    const u32 tiles = ceil_div(n, SORT_TILE);
+    u64 *src = keys, *dst = tmp;
+    for (int p = 0; p < np; p++) {
+        const int d = digits[p];
+        if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * RADIX * sizeof(u32), s))) return false;
+        onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
+                                                       ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);
+        if (!CGB_CUDA(cudaGetLastError())) return false;
+        std::swap(src, dst);
+    }
+    *sorted = src;
+    if (stats) {
+        stats->passes = np;
+        stats->n = n;
+    }
+    return check_err(ws, s, "sort_keys");
+}
+
+bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s)
+{
+    *n_out = 0;
+    if (n == 0) return true;
+    if (n > (u64)LB_MASK) {
+        set_error("unique_keys: more than 2^30 keys in one call");
+        return false;
+    }
+    if (!ws.reserve(n, s)) return false;
+    const u32 tiles = ceil_div(n, UNQ_TILE);
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * sizeof(u32), s))) return false;
+    unique_kernel<<<tiles, UNQ_THREADS, 0, s>>>(in, (u32)n, out, ws.lookback, ws.small + W_CTR,
+                                                ws.small + W_COUNT, ws.small + W_ERR);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    u32 cnt = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!check_err(ws, s, "unique_keys")) return false;
+    *n_out = cnt;
+    return true;
+}
+
+bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_out, SortWorkspace &ws,
+                  cudaStream_t s)
+{
+    *n_out = 0;
+    const u64 total = na + nb;
+    if (total == 0) return true;
+    if (total > (u64)LB_MASK) {
+        set_error("merge_unique: more than 2^30 keys in one call");
+        return false;
+    }
+    if (!ws.reserve(total, s)) return false;
+    const u32 tiles = ceil_div(total, MRG_TILE);
+    // splits live after the look-back words
+    u32 *splits = ws.lookback + ((u64)tiles + 1);
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, ((u64)tiles + 1) * sizeof(u32), s))) return false;
+    merge_partition_kernel<<<ceil_div(tiles + 1, 256), 256, 0, s>>>(a, (u32)na, b, (u32)nb, splits, tiles);
+    merge_unique_kernel<<<tiles, MRG_THREADS, 0, s>>>(a, (u32)na, b, (u32)nb, splits, out, ws.lookback,
+                                                      ws.small + W_CTR, ws.small + W_COUNT, ws.small + W_ERR);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    u32 cnt = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!check_err(ws, s, "merge_unique")) return false;
+    *n_out = cnt;
+    return true;
+}
+
+}  // namespace cgb

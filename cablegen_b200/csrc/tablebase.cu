@@ -1,0 +1,429 @@
+// tablebase.cu -- the C ABI of the engine (include/cablegen_b200.h).
+#include "cgb_engine.h"
+#include <algorithm>
+#include <map>
+#include <vector>
+
+using namespace cgb;
+
+namespace cgb {
+
+// the 8 images of a winstate (get_all_rots, src/board.c:349-374)
+std::vector<u64> expand_winstates(const u64 *w, int n)
+{
+    std::vector<u64> out;
+    for (int i = 0; i < n; i++) {
+        const u64 b = w[i], f = flip_v(b);
+        const u64 imgs[8] = {b, rot_cw(b), rot_cw(rot_cw(b)), rot_ccw(b),
+                             f, rot_cw(f), rot_cw(rot_cw(f)), rot_ccw(f)};
+        for (u64 x : imgs) out.push_back(x);
+    }
+    return out;
+}
+
+SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws)
+{
+    SolveRules s;
+    s.nox = (int)(signed char)r.nox;  // the solver keeps nox in a char (src/solve.c:18)
+    s.score = r.score ? 1 : 0;
+    s.winstates = d_ws;
+    s.n_winstates = nws;
+    return s;
+}
+
+// pinned staging for device -> host copies of layers and tables
+struct HostStage {
+    void *p = nullptr;
+    u64 bytes = 0;
+    bool reserve(u64 b)
+    {
+        if (b <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        if (!CGB_CUDA(cudaMallocHost(&p, b))) return false;
+        bytes = b;
+        return true;
+    }
+    ~HostStage()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+}  // namespace cgb
+
+static Engine &E() { return Engine::get(); }
+
+#define CGB_TRY(x)      \
+    do {                \
+        if (!(x)) return -1; \
+    } while (0)
+
+extern "C" {
+
+const char *cgb_last_error(void) { return last_error(); }
+
+int cgb_init(int device)
+{
+    CGB_TRY(E().init(device));
+    return 0;
+}
+
+static bool ensure_init()
+{
+    if (E().ready) return true;
+    return E().init(0);
+}
+
+int cgb_set_rules(const cgb_rules *r)
+{
+    CGB_TRY(ensure_init());
+    CGB_TRY(E().set_rules(*r));
+    return 0;
+}
+
+static bool ensure_rules()
+{
+    if (!ensure_init()) return false;
+    if (E().rt.move) return true;
+    cgb_rules r{};
+    r.stsl = 200;
+    r.ltc = 5;
+    r.smallest_large = 6;
+    return E().set_rules(r);
+}
+
+int cgb_expand_moves(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t cap, uint64_t *n_out)
+{
+    CGB_TRY(ensure_rules());
+    if (cap < 4 * n) {
+        set_error("cgb_expand_moves: the output needs 4n slots");
+        return -1;
+    }
+    CGB_TRY(expand_moves(d_in, n, d_out, cap, n_out, E().rt, E().prune_params(), E().ctr, E().stream));
+    return 0;
+}
+
+int cgb_count_spawns(const uint64_t *d_in, uint64_t n, uint64_t *total)
+{
+    CGB_TRY(ensure_init());
+    CGB_TRY(count_spawns(d_in, n, total, E().ctr, E().stream));
+    return 0;
+}
+
+int cgb_expand_spawns(const uint64_t *d_in, uint64_t n, uint64_t *d_out2, uint64_t *d_out4, uint64_t cap,
+                      uint64_t *n_out)
+{
+    CGB_TRY(ensure_init());
+    CGB_TRY(expand_spawns(d_in, n, d_out2, d_out4, cap, n_out, E().ctr, E().stream));
+    return 0;
+}
+
+int cgb_sort(uint64_t *d_keys, uint64_t *d_tmp, uint64_t n, int *result_in_tmp, int *passes)
+{
+    CGB_TRY(ensure_init());
+    u64 *sorted = nullptr;
+    SortStats st;
+    CGB_TRY(sort_keys(d_keys, d_tmp, n, &sorted, E().ws, E().stream, &st));
+    CGB_TRY(E().sync());
+    if (result_in_tmp) *result_in_tmp = (sorted == d_tmp) ? 1 : 0;
+    if (passes) *passes = st.passes;
+    return 0;
+}
+
+int cgb_unique(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *n_out)
+{
+    CGB_TRY(ensure_init());
+    CGB_TRY(unique_keys(d_in, n, d_out, n_out, E().ws, E().stream));
+    return 0;
+}
+
+int cgb_merge_unique(const uint64_t *d_a, uint64_t na, const uint64_t *d_b, uint64_t nb, uint64_t *d_out,
+                     uint64_t *n_out)
+{
+    CGB_TRY(ensure_init());
+    CGB_TRY(merge_unique(d_a, na, d_b, nb, d_out, n_out, E().ws, E().stream));
+    return 0;
+}
+
+}  // extern "C"
+
+__global__ void canonicalize_kernel(const u64 *__restrict__ in, u64 n, u64 *__restrict__ out)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        out[i] = canonical(in[i]);
+}
+
+extern "C" int cgb_canonicalize(const uint64_t *d_in, uint64_t n, uint64_t *d_out)
+{
+    CGB_TRY(ensure_init());
+    if (n == 0) return 0;
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
+    canonicalize_kernel<<<grid, 256, 0, E().stream>>>(d_in, n, d_out);
+    CGB_TRY(CGB_CUDA(cudaGetLastError()));
+    CGB_TRY(E().sync());
+    return 0;
+}
+
+extern "C" int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, int precision,
+                               const uint64_t *d_k2, const void *d_v2, uint64_t n2, const uint64_t *d_k4,
+                               const void *d_v4, uint64_t n4, const uint64_t *h_winstates, int n_winstates)
+{
+    CGB_TRY(ensure_rules());
+    cudaStream_t s = E().stream;
+    std::vector<u64> ws = expand_winstates(h_winstates, n_winstates);
+    u64 *d_ws = nullptr;
+    CGB_TRY(dev_alloc((void **)&d_ws, ws.size() * 8 + 8, s));
+    if (!ws.empty())
+        CGB_TRY(CGB_CUDA(cudaMemcpyAsync(d_ws, ws.data(), ws.size() * 8, cudaMemcpyHostToDevice, s)));
+    LayerIndex t2, t4;
+    t2.keys = d_k2;
+    t2.vals = d_v2;
+    t2.n = n2;
+    t4.keys = d_k4;
+    t4.vals = d_v4;
+    t4.n = n4;
+    const SolveRules r = make_solve_rules(E().rules, d_ws, (int)ws.size());
+    bool ok;
+    if (precision == 32)
+        ok = solve_layer_f32(d_keys, n, (float *)d_out, t2, t4, r, E().rt, E().ctr, s);
+    else
+        ok = solve_layer_f64(d_keys, n, (double *)d_out, t2, t4, r, E().rt, E().ctr, s);
+    dev_free(d_ws, s);
+    CGB_TRY(ok);
+    CGB_TRY(E().sync());
+    return 0;
+}
+
+// ---------------------------------------------------------------- sweeps
+namespace {
+
+struct CopyOutSink : LayerSink {
+    cgb_layer_fn fn = nullptr;
+    void *user = nullptr;
+    HostStage stage;
+    u64 d2h = 0;
+    bool failed = false;
+    bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
+    {
+        *kept = false;
+        if (!fn) return true;
+        if (!stage.reserve(n * 8 + 8)) return false;
+        if (n && !CGB_CUDA(cudaMemcpyAsync(stage.p, d, n * 8, cudaMemcpyDeviceToHost, s))) return false;
+        if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+        d2h += n * 8;
+        if (fn(user, sum, (const u64 *)stage.p, n) != 0) {
+            set_error("layer callback failed");
+            return false;
+        }
+        return true;
+    }
+};
+
+struct Layer {
+    int sum;
+    DevBuf<u64> keys;
+};
+
+struct KeepSink : LayerSink {
+    std::vector<Layer> layers;
+    cgb_layer_fn fn = nullptr;
+    void *user = nullptr;
+    HostStage stage;
+    u64 d2h = 0;
+    bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
+    {
+        Layer L;
+        L.sum = sum;
+        L.keys.p = d;
+        L.keys.n = n;
+        L.keys.cap = n;
+        layers.push_back(L);
+        *kept = true;
+        if (fn) {
+            if (!stage.reserve(n * 8 + 8)) return false;
+            if (n && !CGB_CUDA(cudaMemcpyAsync(stage.p, d, n * 8, cudaMemcpyDeviceToHost, s))) return false;
+            if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+            d2h += n * 8;
+            if (fn(user, sum, (const u64 *)stage.p, n) != 0) {
+                set_error("layer callback failed");
+                return false;
+            }
+        }
+        return true;
+    }
+};
+
+void fill_gen_stats(cgb_stats *st, const GenTimes &tm)
+{
+    if (!st) return;
+    st->boards_generated += tm.boards;
+    st->expand_ms += tm.expand_ms;
+    st->sort_ms += tm.sort_ms;
+    st->unique_ms += tm.unique_ms;
+    st->merge_ms += tm.merge_ms;
+    st->sorted_keys += tm.sorted_keys;
+    st->sort_key_passes += tm.sort_passes;
+}
+
+}  // namespace
+
+extern "C" int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, int end, cgb_layer_fn fn, void *user,
+                            cgb_stats *stats)
+{
+    CGB_TRY(ensure_rules());
+    CopyOutSink sink;
+    sink.fn = fn;
+    sink.user = user;
+    GenTimes tm;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, E().stream);
+    const bool ok = E().generate(h_initial, n, start, end, sink, &tm);
+    cudaEventRecord(b, E().stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (stats) {
+        *stats = cgb_stats{};
+        fill_gen_stats(stats, tm);
+        stats->gen_ms = ms;
+        stats->total_ms = ms;
+        stats->h2d_bytes = n * 8;
+        stats->d2h_bytes = sink.d2h;
+        stats->layers = (end >= start) ? (u64)((end - start) / 2 + 1) : 0;
+    }
+    CGB_TRY(ok);
+    return 0;
+}
+
+extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, int end_gen, int end_solve,
+                             const uint64_t *h_winstates, int n_winstates, int precision, cgb_layer_fn layer_fn,
+                             cgb_table_fn table_fn, void *user, cgb_stats *stats)
+{
+    CGB_TRY(ensure_rules());
+    Engine &e = E();
+    cudaStream_t s = e.stream;
+    if (stats) *stats = cgb_stats{};
+    KeepSink sink;
+    sink.fn = layer_fn;
+    sink.user = user;
+    GenTimes tm;
+    cudaEvent_t ev[3];
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], s);
+    bool ok = e.generate(h_initial, n, start, end_gen, sink, &tm);
+    cudaEventRecord(ev[1], s);
+
+    // ---- solve, top-down (src/solve.c:203-219) ----
+    std::map<int, size_t> by_sum;
+    for (size_t i = 0; i < sink.layers.size(); i++) by_sum[sink.layers[i].sum] = i;
+    std::vector<u64> ws = expand_winstates(h_winstates, n_winstates);
+    u64 *d_ws = nullptr;
+    const int vbytes = precision == 32 ? 4 : 8;
+    struct Solved {
+        int sum = 0;
+        const u64 *keys = nullptr;
+        void *vals = nullptr;
+        u64 n = 0;
+        u32 *bucket = nullptr;
+        u64 bucket_cap = 0;
+        LayerIndex ix;
+    };
+    Solved t2, t4, cur;
+    HostStage stage;
+    double solve_kernel_ms = 0, index_ms = 0;
+    u64 solved = 0, d2h = sink.d2h;
+    if (ok) ok = dev_alloc((void **)&d_ws, ws.size() * 8 + 8, s);
+    if (ok && !ws.empty()) ok = CGB_CUDA(cudaMemcpyAsync(d_ws, ws.data(), ws.size() * 8, cudaMemcpyHostToDevice, s));
+    const SolveRules rules = make_solve_rules(e.rules, d_ws, (int)ws.size());
+    const int lo = std::max(end_solve, 0);
+    for (int sum = end_gen; ok && sum >= lo && sum > 0; sum -= 2) {
+        auto it = by_sum.find(sum);
+        cur = Solved{};
+        cur.sum = sum;
+        if (it != by_sum.end()) {
+            cur.keys = sink.layers[it->second].keys.p;
+            cur.n = sink.layers[it->second].keys.n;
+        }
+        if (!dev_alloc(&cur.vals, cur.n * vbytes + 8, s)) {
+            ok = false;
+            break;
+        }
+        {
+            Timer t(s, &solve_kernel_ms);
+            if (precision == 32)
+                ok = solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, rules, e.rt, e.ctr, s);
+            else
+                ok = solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, rules, e.rt, e.ctr, s);
+        }
+        if (!ok) break;
+        solved += cur.n;
+        if (table_fn) {
+            const u64 bytes = cur.n * (8 + vbytes);
+            if (!stage.reserve(bytes + 16)) {
+                ok = false;
+                break;
+            }
+            if (cur.n) {
+                ok = CGB_CUDA(cudaMemcpyAsync(stage.p, cur.keys, cur.n * 8, cudaMemcpyDeviceToHost, s)) &&
+                     CGB_CUDA(cudaMemcpyAsync((char *)stage.p + cur.n * 8, cur.vals, cur.n * vbytes,
+                                              cudaMemcpyDeviceToHost, s));
+            }
+            ok = ok && CGB_CUDA(cudaStreamSynchronize(s));
+            if (!ok) break;
+            d2h += bytes;
+            if (table_fn(user, sum, (const u64 *)stage.p, (const char *)stage.p + cur.n * 8, cur.n, precision)) {
+                set_error("table callback failed");
+                ok = false;
+                break;
+            }
+        }
+        cur.ix.keys = cur.keys;
+        cur.ix.vals = cur.vals;
+        cur.ix.n = cur.n;
+        {
+            Timer t(s, &index_ms);
+            ok = build_index(cur.ix, &cur.bucket, &cur.bucket_cap, 0, s);
+        }
+        // the s+4 table is no longer needed: free its values, bucket and keys
+        if (t4.vals) dev_free(t4.vals, s);
+        if (t4.bucket) dev_free(t4.bucket, s);
+        {
+            auto it4 = by_sum.find(t4.sum);
+            if (t4.sum && it4 != by_sum.end()) drop(sink.layers[it4->second].keys, s);
+        }
+        t4 = t2;
+        t2 = cur;
+    }
+    for (Solved *x : {&t2, &t4}) {
+        if (x->vals) dev_free(x->vals, s);
+        if (x->bucket) dev_free(x->bucket, s);
+    }
+    for (auto &L : sink.layers) drop(L.keys, s);
+    dev_free(d_ws, s);
+    cudaEventRecord(ev[2], s);
+    cudaEventSynchronize(ev[2]);
+    float gen_ms = 0, solve_ms = 0;
+    cudaEventElapsedTime(&gen_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&solve_ms, ev[1], ev[2]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (stats) {
+        fill_gen_stats(stats, tm);
+        stats->layers = sink.layers.size();
+        stats->boards_solved = solved;
+        stats->gen_ms = gen_ms;
+        stats->solve_ms = solve_ms;
+        stats->total_ms = gen_ms + solve_ms;
+        stats->solve_kernel_ms = solve_kernel_ms;
+        stats->index_ms = index_ms;
+        stats->h2d_bytes = n * 8;
+        stats->d2h_bytes = d2h;
+    }
+    CGB_TRY(ok);
+    return 0;
+}

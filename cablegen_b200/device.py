@@ -1,0 +1,184 @@
+"""Device-level entry points of the engine on torch CUDA tensors.
+
+Boards live in int64 tensors (the same 64 bits as the reference's uint64_t).
+Every call hands raw device pointers to the C ABI (include/cablegen_b200.h),
+which runs on the engine's own CUDA stream and returns only when its work is
+complete; torch's current stream is synchronised before each call so inputs
+written by torch are visible.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib
+from .configs import Settings
+
+
+def _ptr(t: torch.Tensor):
+    assert t.is_cuda and t.is_contiguous()
+    return C.c_void_p(t.data_ptr())
+
+
+def _sync():
+    torch.cuda.current_stream().synchronize()
+
+
+def init(device: int = 0):
+    check(lib().cgb_init(device))
+
+
+def set_rules(settings: Settings):
+    r = _lib.Rules(int(settings.free_formation), int(settings.ignore_f), int(settings.prune), settings.stsl,
+                   settings.ltc, settings.smallest_large, settings.nox, int(settings.score))
+    check(lib().cgb_set_rules(C.byref(r)))
+
+
+def to_device(a, device="cuda") -> torch.Tensor:
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+    return torch.from_numpy(a.view(np.int64)).to(device)
+
+
+def to_numpy(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().numpy().view(np.uint64)
+
+
+def empty(n: int, device="cuda") -> torch.Tensor:
+    return torch.empty(max(int(n), 1), dtype=torch.int64, device=device)
+
+
+def canonicalize(x: torch.Tensor) -> torch.Tensor:
+    _sync()
+    out = empty(x.numel())
+    check(lib().cgb_canonicalize(_ptr(x), x.numel(), _ptr(out)))
+    return out[: x.numel()]
+
+
+def expand_moves(x: torch.Tensor) -> torch.Tensor:
+    _sync()
+    n = x.numel()
+    out = empty(4 * n)
+    cnt = C.c_uint64()
+    check(lib().cgb_expand_moves(_ptr(x), n, _ptr(out), 4 * n, C.byref(cnt)))
+    return out[: cnt.value]
+
+
+def count_spawns(x: torch.Tensor) -> int:
+    _sync()
+    tot = C.c_uint64()
+    check(lib().cgb_count_spawns(_ptr(x), x.numel(), C.byref(tot)))
+    return tot.value
+
+
+def expand_spawns(x: torch.Tensor) -> Tuple[torch.Tensor, torch.Tensor]:
+    total = count_spawns(x)
+    o2, o4 = empty(total), empty(total)
+    cnt = C.c_uint64()
+    check(lib().cgb_expand_spawns(_ptr(x), x.numel(), _ptr(o2), _ptr(o4), total, C.byref(cnt)))
+    return o2[: cnt.value], o4[: cnt.value]
+
+
+def sort(x: torch.Tensor) -> Tuple[torch.Tensor, int]:
+    """Ascending unsigned sort; returns (sorted tensor, digit passes)."""
+    _sync()
+    keys = x.clone()
+    tmp = empty(x.numel())
+    in_tmp, passes = C.c_int(), C.c_int()
+    check(lib().cgb_sort(_ptr(keys), _ptr(tmp), x.numel(), C.byref(in_tmp), C.byref(passes)))
+    return (tmp if in_tmp.value else keys)[: x.numel()], passes.value
+
+
+def unique(x_sorted: torch.Tensor) -> torch.Tensor:
+    _sync()
+    out = empty(x_sorted.numel())
+    cnt = C.c_uint64()
+    check(lib().cgb_unique(_ptr(x_sorted), x_sorted.numel(), _ptr(out), C.byref(cnt)))
+    return out[: cnt.value]
+
+
+def sort_unique(x: torch.Tensor) -> torch.Tensor:
+    s, _ = sort(x)
+    return unique(s)
+
+
+def merge_unique(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    _sync()
+    out = empty(a.numel() + b.numel())
+    cnt = C.c_uint64()
+    check(lib().cgb_merge_unique(_ptr(a) if a.numel() else None, a.numel(), _ptr(b) if b.numel() else None,
+                                 b.numel(), _ptr(out), C.byref(cnt)))
+    return out[: cnt.value]
+
+
+def solve_layer(keys: torch.Tensor, t2: Tuple[torch.Tensor, torch.Tensor], t4: Tuple[torch.Tensor, torch.Tensor],
+                winstates: Sequence[int], precision: int = 64) -> torch.Tensor:
+    _sync()
+    dt = torch.float64 if precision == 64 else torch.float32
+    out = torch.empty(max(keys.numel(), 1), dtype=dt, device=keys.device)
+    ws = (C.c_uint64 * max(len(winstates), 1))(*[int(w) for w in winstates])
+
+    def p(t):
+        return _ptr(t) if t is not None and t.numel() else None
+
+    check(lib().cgb_solve_layer(p(keys), keys.numel(), _ptr(out), precision, p(t2[0]), p(t2[1]), t2[0].numel(),
+                                p(t4[0]), p(t4[1]), t4[0].numel(), ws, len(winstates)))
+    return out[: keys.numel()]
+
+
+def generate(initial: Sequence[int], start: int, end: int, keep: bool = True):
+    """Generation sweep; returns ({sum: numpy layer}, stats dict)."""
+    layers: Dict[int, np.ndarray] = {}
+
+    def on_layer(user, s, ptr, n):
+        if keep:
+            layers[s] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+        return 0
+
+    cb = _lib.LAYER_FN(on_layer)
+    init_a = (C.c_uint64 * max(len(initial), 1))(*[int(b) for b in initial])
+    st = _lib.Stats()
+    check(lib().cgb_generate(init_a, len(initial), start, end, cb, None, C.byref(st)))
+    return layers, st.as_dict()
+
+
+def tablebase(initial: Sequence[int], start: int, end_gen: int, end_solve: int, winstates: Sequence[int],
+              precision: int = 64, keep_layers: bool = False, keep_tables: bool = False,
+              layer_fn=None, table_fn=None):
+    """Generation + solve with layers resident in HBM.
+
+    Returns (layers, tables, stats): layers {sum: keys}, tables {sum: (keys, values)} when kept.
+    """
+    layers, tables = {}, {}
+
+    def on_layer(user, s, ptr, n):
+        if keep_layers:
+            layers[s] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+        if layer_fn is not None:
+            layer_fn(s, ptr, n)
+        return 0
+
+    def on_table(user, s, kptr, vptr, n, prec):
+        if keep_tables:
+            k = np.ctypeslib.as_array(kptr, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+            vt = C.c_double if prec == 64 else C.c_float
+            v = (np.ctypeslib.as_array(C.cast(vptr, C.POINTER(vt)), shape=(n,)).copy() if n
+                 else np.zeros(0, np.float64 if prec == 64 else np.float32))
+            tables[s] = (k, v)
+        if table_fn is not None:
+            table_fn(s, kptr, vptr, n, prec)
+        return 0
+
+    want_layers = keep_layers or layer_fn is not None
+    want_tables = keep_tables or table_fn is not None
+    lcb = _lib.LAYER_FN(on_layer) if want_layers else _lib.LAYER_FN()
+    tcb = _lib.TABLE_FN(on_table) if want_tables else _lib.TABLE_FN()
+    init_a = (C.c_uint64 * max(len(initial), 1))(*[int(b) for b in initial])
+    ws = (C.c_uint64 * max(len(winstates), 1))(*[int(w) for w in winstates])
+    st = _lib.Stats()
+    check(lib().cgb_tablebase(init_a, len(initial), start, end_gen, end_solve, ws, len(winstates), precision,
+                              lcb, tcb, None, C.byref(st)))
+    return layers, tables, st.as_dict()

@@ -1,0 +1,105 @@
+/*
+ * cablegen_b200.h -- C ABI of the B200 engine below the cablegen API.
+ *
+ * Plain pointers and sizes only.  Functions return 0 on success and -1 on
+ * failure; cgb_last_error() then describes the failure.  "d_" pointers are
+ * device memory of the current CUDA device, "h_" pointers host memory.
+ * Boards are u64 (nibble 0 = top-left cell, api/cablegen.h:9-12).
+ *
+ * The library is single-caller like the reference (global state: the row
+ * table, settings); calls are serialised on one internal CUDA stream.
+ */
+#ifndef CABLEGEN_B200_H
+#define CABLEGEN_B200_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Generation/solve knobs (src/settings.c:34-59, settings.h:15-31). */
+typedef struct {
+    int free_formation;        /* [Cablegen] free_formation */
+    int ignore_f;              /* [Cablegen] ignore_f */
+    int prune;                 /* [Generate] prune */
+    long long stsl;            /* [Generate] stsl */
+    long long ltc;             /* [Generate] ltc */
+    long long smallest_large;  /* [Generate] smallest_large */
+    int nox;                   /* [Cablegen] nox (char semantics: solve.c:18) */
+    int score;                 /* [Solve] score */
+} cgb_rules;
+
+/* Initialise the engine on a device; idempotent. */
+int cgb_init(int device);
+const char *cgb_last_error(void);
+/* Build and upload the row table for these rules (generate_lut, src/board.c:100-132). */
+int cgb_set_rules(const cgb_rules *rules);
+
+/* ---- device primitives of one layer step --------------------------------
+ * Move + prune + canonicalise every board (the move workers,
+ * src/generate.c:133-175; OpenCL move_kernel, src/cl/generate.cl:249-282).
+ * d_out needs cap >= 4n slots; *n_out = boards written (unsorted). */
+int cgb_expand_moves(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t cap, uint64_t *n_out);
+/* Total number of empty cells (= size of each spawn stream). */
+int cgb_count_spawns(const uint64_t *d_in, uint64_t n, uint64_t *total);
+/* Canonical 2- and 4-spawns of every empty cell (src/generate.c:177-199). */
+int cgb_expand_spawns(const uint64_t *d_in, uint64_t n, uint64_t *d_out2, uint64_t *d_out4, uint64_t cap,
+                      uint64_t *n_out);
+/* Ascending LSD radix sort of d_keys[0,n) with scratch d_tmp[0,n) (replaces
+ * qs_sort_h/fluxsort_uint64, src/array.c:289-291).  *result_in_tmp tells which
+ * buffer holds the result; *passes = digit passes executed. */
+int cgb_sort(uint64_t *d_keys, uint64_t *d_tmp, uint64_t n, int *result_in_tmp, int *passes);
+/* Drop repeats of a sorted array into d_out (must not alias d_in). */
+int cgb_unique(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *n_out);
+/* Sorted union without repeats of two sorted unique arrays
+ * (deduplicate_threads with two runs, src/array.c:246-287). */
+int cgb_merge_unique(const uint64_t *d_a, uint64_t na, const uint64_t *d_b, uint64_t nb, uint64_t *d_out,
+                     uint64_t *n_out);
+/* Canonical form of every board (canonicalize_b, src/board.c:314-337). */
+int cgb_canonicalize(const uint64_t *d_in, uint64_t n, uint64_t *d_out);
+
+/* ---- solve of one layer (solve_layer, src/solve.c:289-340) ---------------
+ * precision 64: d_out/d_v2/d_v4 are double; 32: float (Kahan sums).
+ * (d_k2,d_v2,n2) and (d_k4,d_v4,n4): the s+2 and s+4 tables, keys sorted.
+ * h_winstates: winstate patterns, expanded to all 8 symmetries inside. */
+int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, int precision, const uint64_t *d_k2,
+                    const void *d_v2, uint64_t n2, const uint64_t *d_k4, const void *d_v4, uint64_t n4,
+                    const uint64_t *h_winstates, int n_winstates);
+
+/* ---- whole sweeps -------------------------------------------------------- */
+typedef struct {
+    uint64_t layers, boards_generated, boards_solved;
+    double gen_ms, solve_ms, total_ms;         /* device time (CUDA events) */
+    double expand_ms, sort_ms, unique_ms, merge_ms, solve_kernel_ms, index_ms;
+    uint64_t sorted_keys, sort_key_passes;     /* keys through the sort, keys x passes */
+    uint64_t lookups_bytes;                    /* algorithmic bytes of the solve kernels */
+    uint64_t h2d_bytes, d2h_bytes;
+    double max_abs_err;                        /* fp32 runs with check: max |fp32 - fp64| */
+    uint64_t gpu_launches;                     /* kernels launched by the library */
+} cgb_stats;
+
+/* Layer callback: the layer `sum` as a host array (valid during the call). */
+typedef int (*cgb_layer_fn)(void *user, int sum, const uint64_t *h_boards, uint64_t n);
+/* Table callback: keys and values (double, or float for precision 32). */
+typedef int (*cgb_table_fn)(void *user, int sum, const uint64_t *h_keys, const void *h_values, uint64_t n,
+                            int precision);
+
+/* Generation sweep from h_initial (all of tile sum `start`) up to `end`
+ * (generate(), src/generate.c:551-615); every layer goes to fn. */
+int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, int end, cgb_layer_fn fn, void *user,
+                 cgb_stats *stats);
+
+/* Generation + solve with every layer resident in HBM (generate() then
+ * solve(), src/solve.c:172-224, without files).  Layers are solved from
+ * end_gen down to max(end_solve, start).  precision 64 or 32.  When
+ * layer_fn / table_fn are non-null every layer / table is copied to the host
+ * and handed to them (the end-to-end path). */
+int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, int end_gen, int end_solve,
+                  const uint64_t *h_winstates, int n_winstates, int precision, cgb_layer_fn layer_fn,
+                  cgb_table_fn table_fn, void *user, cgb_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,72 @@
+"""Whole sweeps on the GPU against the reference's own layer and table digests."""
+import numpy as np
+import pytest
+
+import py_oracle as O
+from cablegen_b200 import configs
+from helpers import digests, sha_layer, sha_table
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["plain_2x4", "plain_2x4_nearwall"])
+def test_generate_matches_reference(cuda, name):
+    w = configs.get(name)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    layers, st = cuda.generate(f.initial, f.start, f.end_gen)
+    d = digests(name)["layers"]
+    assert sorted(int(s) for s in d) == sorted(layers)
+    for s, rec in d.items():
+        assert len(layers[int(s)]) == rec["boards"], s
+        assert sha_layer(layers[int(s)]) == rec["boards_sha256"], s
+    assert st["boards_generated"] == sum(r["boards"] for r in d.values())
+
+
+@pytest.mark.parametrize("name", ["plain_2x4", "plain_2x4_nearwall"])
+def test_tablebase_fp64_bit_exact(cuda, name):
+    w = configs.get(name)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    layers, tables, st = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=64,
+                                        keep_layers=True, keep_tables=True)
+    d = digests(name)["layers"]
+    for s, rec in d.items():
+        k, v = tables[int(s)]
+        assert sha_table(k, v) == rec["tables_sha256"], s
+    # layers below the initial sum are solved as empty tables (solve.c:203-211)
+    assert all(len(tables[s][0]) == 0 for s in tables if s < f.start)
+
+
+def test_tablebase_fp32_error(cuda):
+    w = configs.get("plain_2x4_nearwall")
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    _, t64, _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=64, keep_tables=True)
+    _, t32, _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=32, keep_tables=True)
+    err = max((np.abs(t64[s][1] - t32[s][1].astype(np.float64)).max() if len(t64[s][1]) else 0.0) for s in t64)
+    assert err <= 1e-6, err
+
+
+def test_solve_layer_matches_oracle(cuda):
+    """One layer through cgb_solve_layer against the oracle, with nox and score variants."""
+    w = configs.get("plain_2x4_nearwall")
+    f = w.formations[0]
+    lut = O.make_lut(0, 0)
+    layers = O.generate(lut, O.settings(w.settings), f.initial, f.start, 60)
+    for nox, score in ((0, 0), (5, 0), (0, 1)):
+        st = configs.Settings(nox=nox, score=bool(score))
+        cuda.set_rules(st)
+        ost = O.settings(st)
+        ws = O.expand_winstates(f.winstates)
+        t4 = (layers[60], O.solve_layer(lut, ost, layers[60], (np.zeros(0, np.uint64),) * 2, (np.zeros(0, np.uint64),) * 2, ws))
+        t2 = (layers[58], O.solve_layer(lut, ost, layers[58], t4, (np.zeros(0, np.uint64),) * 2, ws))
+        want = O.solve_layer(lut, ost, layers[56], t2, t4, ws)
+        got = cuda.solve_layer(cuda.to_device(layers[56]), (cuda.to_device(t2[0]), _f(cuda, t2[1])),
+                               (cuda.to_device(t4[0]), _f(cuda, t4[1])), f.winstates, 64)
+        assert np.array_equal(got.cpu().numpy(), want), (nox, score)
+
+
+def _f(cuda, v):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).cuda()
