@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark: boards/s of tablebase generation + solve on B200.
+
+Workload (default): the LL/4422 pruned configuration -- 64 seeded 4-tile
+boards, prune stsl=58 ltc=5 smallest_large=6, generation from the initial tile
+sum up to 600, then the plain FP64 solve from 600 back down, 256 goal in the
+top-left.  One step = one complete generation + solve sweep with every layer
+resident in HBM (layers total tens of GB, far above L2, so no flush is needed
+between steps).  value = (boards generated + boards solved) / device time.
+
+Also reported on the same line:
+  fp32     -- the same sweep with FP32 tables and Kahan spawn sums, its
+              throughput and its max-abs error against the FP64 tables
+  e2e      -- the sweep through the C ABI with every layer and table copied
+              to host buffers inside the timed region
+  roofline -- the dominant kernel's algorithmic bytes / its CUDA-event time
+  cpu_baseline -- the reference's own CPU code on a bounded sample
+
+`--impl reference` runs the reference's CPU implementation (oracle/_ref/cli,
+built from the reference sources) on a bounded sample of the same workload.
+Multi-GPU: every rank runs an independent replica (the generator has no
+cross-GPU exchange); value is the sum over ranks / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Boards/s gen+solve, FP32 vs FP64 solve at <=1e-6 err; lookup/sort HBM GB/s"
+REF_CLI = os.path.join(ROOT, "oracle", "_ref", "cli")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ll_pruned")
+    ap.add_argument("--end", type=int, default=None, help="override the workload's end tile sum")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-end", type=int, default=None, help="end tile sum of the CPU sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- helpers
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 10:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return self.summary()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        load = [s for s in self.samples if (num(s[9]) or 0) > 10] or self.samples
+        sm = [num(s[1]) for s in load if num(s[1]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in load:
+            for name, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(self.samples[0][2]),
+                "power_w_max": max((num(s[3]) or 0) for s in self.samples),
+                "samples": len(self.samples), "samples_under_load": len(load),
+                "reasons": sorted(reasons)}
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- CPU baseline (reference build)
+def reference_sample(workload, end, cores, workdir=None):
+    """Run the reference CLI (generate then solve) on the workload's first layers.
+
+    Returns (boards processed, seconds, description).  The reference refuses
+    more than 127 worker threads (src/array.c:247-251).
+    """
+    from cablegen_b200 import configs
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import write_conf
+    import numpy as np
+    wl = configs.get(workload)
+    form = wl.formations[0]
+    cores = max(1, min(cores, 127))
+    work = workdir or tempfile.mkdtemp(prefix="cgref_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        bdir = os.path.join(work, "boards") + "/"
+        tdir = os.path.join(work, "tables") + "/"
+        os.makedirs(bdir, exist_ok=True)
+        os.makedirs(tdir, exist_ok=True)
+        np.array(form.initial, dtype="<u8").tofile(os.path.join(work, "initial"))
+        np.array(form.winstates, dtype="<u8").tofile(os.path.join(work, "winstates"))
+        conf = os.path.join(work, "cablegen.conf")
+        write_conf(conf, wl, form, bdir, tdir, cores, end_gen=end, end_solve=form.start)
+        env = dict(os.environ, XDG_CONFIG_HOME=work)
+        t0 = time.perf_counter()
+        subprocess.run([REF_CLI, f"-C={conf}", f"-c={cores}", "generate"], check=True, cwd=work,
+                       stdout=subprocess.DEVNULL, env=env)
+        gen_boards = sum(os.path.getsize(os.path.join(bdir, f)) // 8 for f in os.listdir(bdir))
+        subprocess.run([REF_CLI, f"-C={conf}", f"-c={cores}", "solve"], check=True, cwd=work,
+                       stdout=subprocess.DEVNULL, env=env)
+        dt = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    desc = (f"reference CLI (oracle/_ref/cli) -c={cores}: generate {form.start}..{end} then solve {end}..{form.start} "
+            f"of {workload} ({gen_boards} boards each way)")
+    return 2 * gen_boards, dt, desc
+
+
+def default_cpu_end(workload):
+    return {"ll_pruned": 160, "plain_2x4": 300, "dpdf": 340, "ll_large": 100}.get(workload, 120)
+
+
+def run_reference_arm(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    end = args.cpu_end or default_cpu_end(args.workload)
+    if not os.path.exists(REF_CLI):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cli was not built (make -C oracle ref)"}))
+        return 0
+    for _ in range(args.warmup):
+        reference_sample(args.workload, end, cores)
+    boards = 0
+    secs = 0.0
+    desc = ""
+    for _ in range(args.steps):
+        b, dt, desc = reference_sample(args.workload, end, cores)
+        boards += b
+        secs += dt
+    value = boards / secs
+    line = {"metric": METRIC, "value": value, "unit": "boards/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * secs / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 boards)",
+            "impl": "reference",
+            "config": {"workload": args.workload, "sample_end": end, "cores": min(cores, 127)},
+            "cpu_baseline": {"value": value, "unit": "boards/s", "cores": min(cores, 127), "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "boards/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    else:
+        dist = None
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    from cablegen_b200 import configs, device
+    wl = configs.get(args.workload) if args.end is None else configs.get(args.workload, end_gen=args.end)
+    form = wl.formations[0]
+    device.init(dev)
+    device.set_rules(wl.settings)
+
+    def step(precision=64, e2e=False):
+        h = {"d2h": 0}
+        if e2e:
+            def on_layer(s, ptr, n):
+                h["d2h"] += 8 * n
+
+            def on_table(s, kp, vp, n, prec):
+                h["d2h"] += (8 + prec // 8) * n
+            _, _, st = device.tablebase(form.initial, form.start, form.end_gen, form.start, form.winstates,
+                                        precision, layer_fn=on_layer, table_fn=on_table)
+        else:
+            _, _, st = device.tablebase(form.initial, form.start, form.end_gen, form.start, form.winstates,
+                                        precision)
+        return st
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step(64)
+
+    # ---- timed region: K steps of the FP64 sweep
+    barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    device.reset_kernel_stats()
+    t0 = time.perf_counter()
+    stats = [step(64) for _ in range(args.steps)]
+    barrier()
+    wall = time.perf_counter() - t0
+    clock_summary = clocks.stop()
+    kst = device.kernel_stats()
+    dev_ms = sum(s["total_ms"] for s in stats)
+    boards = sum(s["boards_generated"] + s["boards_solved"] for s in stats)
+    gpu_launches = kst["launches"]
+
+    # ---- FP32 sweep and its error against FP64
+    fp32 = None
+    if not args.no_fp32:
+        device.reset_kernel_stats()
+        s32 = step(32)
+        k32 = device.kernel_stats()
+        fp32 = {"value": (s32["boards_generated"] + s32["boards_solved"]) / (s32["total_ms"] / 1000.0),
+                "solve_boards_per_s": s32["boards_solved"] / (k32["solve_ms"] / 1000.0) if k32["solve_ms"] else None,
+                "fp64_solve_boards_per_s": kst["solve_boards"] / (kst["solve_ms"] / 1000.0) if kst["solve_ms"] else None}
+        if fp32["solve_boards_per_s"] and fp32["fp64_solve_boards_per_s"]:
+            fp32["solve_speedup_vs_fp64"] = fp32["solve_boards_per_s"] / fp32["fp64_solve_boards_per_s"]
+
+    # ---- end to end through the C ABI, layers and tables copied to host
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t1 = time.perf_counter()
+        se = [step(64, e2e=True) for _ in range(args.steps)]
+        barrier()
+        e2e_wall = time.perf_counter() - t1
+        e2e_boards = sum(s["boards_generated"] + s["boards_solved"] for s in se)
+        e2e = {"value": e2e_boards / e2e_wall, "unit": "boards/s",
+               "h2d_bytes_per_step": int(se[0]["h2d_bytes"]), "d2h_bytes_per_step": int(se[0]["d2h_bytes"])}
+
+    # ---- aggregate over ranks: sum of boards / slowest rank
+    if dist is not None:
+        t = torch.tensor([boards, dev_ms, wall], dtype=torch.float64, device="cuda")
+        tb = t.clone()
+        dist.all_reduce(tb[0:1], op=dist.ReduceOp.SUM)
+        dist.all_reduce(tb[1:3], op=dist.ReduceOp.MAX)
+        boards_all, dev_ms_max = float(tb[0]), float(tb[1])
+        if e2e is not None:
+            te = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
+            dist.all_reduce(te, op=dist.ReduceOp.MIN)
+            e2e["value"] = float(te[0]) * world
+    else:
+        boards_all, dev_ms_max = boards, dev_ms
+    value = boards_all / (dev_ms_max / 1000.0)
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = hbm_peak()
+    fams = {"onesweep": "sort digit pass (onesweep)", "solve": "solve (expectimax + lookups)",
+            "expand": "move expansion", "spawn": "spawn expansion", "unique": "unique", "merge": "merge",
+            "hist": "sort histogram"}
+    dom = max(fams, key=lambda k: kst[f"{k}_ms"])
+    achieved = kst[f"{dom}_bytes"] / 1e9 / (kst[f"{dom}_ms"] / 1000.0) if kst[f"{dom}_ms"] else 0.0
+    roofline = {"kernel": fams[dom], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "traffic": None,
+                "kernels": {k: {"ms": round(kst[f"{k}_ms"], 3),
+                                "GB/s": round(kst[f"{k}_bytes"] / 1e6 / kst[f"{k}_ms"], 1) if kst[f"{k}_ms"] else None,
+                                "share": round(kst[f"{k}_ms"] / max(dev_ms, 1e-9), 4)}
+                            for k in fams}}
+    roofline["kernels"]["solve"]["lookups"] = kst["lookups"]
+
+    # ---- CPU baseline: the reference build on a bounded sample (rank 0, N=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(REF_CLI):
+        cores = host_cores()
+        end = args.cpu_end or default_cpu_end(args.workload)
+        b, dt, desc = reference_sample(args.workload, end, cores)
+        cpu = {"value": b / dt, "unit": "boards/s", "cores": min(cores, 127), "kind": "reference", "sample": desc}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "boards/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded SplitMix64 initial boards)",
+                "config": {"workload": args.workload, "description": wl.description, "start": form.start,
+                           "end_gen": form.end_gen, "solve": "fp64", "parallelism": f"replicas x{world}",
+                           "boards_per_step": boards // max(args.steps, 1),
+                           "l2": "inputs larger than L2 (layers resident in HBM, tens of GB)"},
+                "wall_s": wall, "gpu_launches": gpu_launches, "clocks": clock_summary, "roofline": roofline,
+                "fp32": fp32, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -41,6 +41,20 @@ class Stats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class KernelStats(C.Structure):
+    """cgb_kernel_stats (include/cablegen_b200.h)."""
+    _fields_ = [("launches", C.c_uint64)] + \
+        [(f"{k}_ms", C.c_double) for k in ("hist", "onesweep", "unique", "merge", "expand", "spawn", "solve",
+                                          "index")] + \
+        [(f"{k}_bytes", C.c_uint64) for k in ("hist", "onesweep", "unique", "merge", "expand", "spawn",
+                                             "solve")] + \
+        [("onesweep_launches", C.c_uint64), ("solve_launches", C.c_uint64), ("solve_boards", C.c_uint64),
+         ("lookups", C.c_uint64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 LAYER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_uint64)
 TABLE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_void_p, C.c_uint64, C.c_int)
 
@@ -63,6 +77,8 @@ def _declare(L):
         "cgb_unique": (C.c_int, [vp, u64, vp, pu64]),
         "cgb_merge_unique": (C.c_int, [vp, u64, vp, u64, vp, pu64]),
         "cgb_canonicalize": (C.c_int, [vp, u64, vp]),
+        "cgb_get_kernel_stats": (C.c_int, [C.POINTER(KernelStats)]),
+        "cgb_reset_kernel_stats": (C.c_int, []),
         "cgb_solve_layer": (C.c_int, [vp, u64, vp, C.c_int, vp, vp, u64, vp, vp, u64, pu64, C.c_int]),
         "cgb_generate": (C.c_int, [pu64, u64, C.c_int, C.c_int, LAYER_FN, vp, C.POINTER(Stats)]),
         "cgb_tablebase": (C.c_int, [pu64, u64, C.c_int, C.c_int, C.c_int, pu64, C.c_int, C.c_int, LAYER_FN,

@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <string>
+#include <vector>
 
 namespace cgb {
 
@@ -32,6 +33,37 @@ bool cuda_ok(cudaError_t e, const char *what, const char *file, int line);
 
 void set_error(const std::string &msg);
 const char *last_error();
+
+// Per-kernel device time and algorithmic bytes, accumulated over launches.
+// Launch time comes from CUDA events recorded around each launch on the
+// launching stream and resolved at the next host synchronisation point.
+struct KernelStats {
+    u64 launches = 0;
+    double hist_ms = 0, onesweep_ms = 0, unique_ms = 0, merge_ms = 0, expand_ms = 0, spawn_ms = 0,
+           solve_ms = 0, index_ms = 0;
+    u64 hist_bytes = 0, onesweep_bytes = 0, unique_bytes = 0, merge_bytes = 0, expand_bytes = 0,
+        spawn_bytes = 0, solve_bytes = 0;
+    u64 onesweep_launches = 0, solve_launches = 0, solve_boards = 0, lookups = 0;
+};
+KernelStats &kstats();
+
+class KClock {
+  public:
+    void begin(cudaStream_t s, double *acc);
+    void end(cudaStream_t s);
+    void flush();  // call after the stream has been synchronised
+  private:
+    struct Pending {
+        cudaEvent_t a, b;
+        double *acc;
+    };
+    cudaEvent_t take();
+    std::vector<cudaEvent_t> free_;
+    std::vector<Pending> pend_;
+    cudaEvent_t open_ = nullptr;
+    double *open_acc_ = nullptr;
+};
+KClock &kclock();
 
 #ifdef __CUDACC__
 __device__ __forceinline__ u32 ld_acquire(const u32 *p)

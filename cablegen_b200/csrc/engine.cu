@@ -53,16 +53,132 @@ std::string err_string(u32 err)
     return s.empty() ? "[none]" : s;
 }
 
+// ---- kernel clocks ----------------------------------------------------------
+KernelStats &kstats()
+{
+    static KernelStats k;
+    return k;
+}
+KClock &kclock()
+{
+    static KClock c;
+    return c;
+}
+cudaEvent_t KClock::take()
+{
+    if (free_.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = free_.back();
+    free_.pop_back();
+    return e;
+}
+void KClock::begin(cudaStream_t s, double *acc)
+{
+    open_ = take();
+    open_acc_ = acc;
+    cudaEventRecord(open_, s);
+    kstats().launches++;
+}
+void KClock::end(cudaStream_t s)
+{
+    if (!open_) return;
+    cudaEvent_t b = take();
+    cudaEventRecord(b, s);
+    pend_.push_back({open_, b, open_acc_});
+    open_ = nullptr;
+}
+void KClock::flush()
+{
+    for (auto &p : pend_) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && p.acc) *p.acc += ms;
+        free_.push_back(p.a);
+        free_.push_back(p.b);
+    }
+    pend_.clear();
+}
+
 // ---- memory -----------------------------------------------------------------
 bool dev_alloc(void **p, u64 bytes, cudaStream_t s)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 256;
-    return CGB_CUDA(cudaMallocAsync(p, bytes, s));
+    cudaError_t e = cudaMallocAsync(p, bytes, s);
+    if (e == cudaErrorMemoryAllocation) {
+        // freed blocks of other sizes may still sit in the pool: return them
+        // to the device and retry once
+        cudaGetLastError();
+        cudaStreamSynchronize(s);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocAsync(p, bytes, s);
+    }
+    if (e != cudaSuccess) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "device allocation of %.3f GB failed: %s", bytes / 1e9, cudaGetErrorString(e));
+        set_error(buf);
+        cudaGetLastError();
+        return false;
+    }
+    return true;
 }
 void dev_free(void *p, cudaStream_t s)
 {
     if (p) cudaFreeAsync(p, s);
+}
+
+// ---- resident layer store ---------------------------------------------------
+u64 *LayerStore::push(u64 n, cudaStream_t s)
+{
+    const u64 need = n ? n : 1;
+    if (chunks_.empty() || chunks_.back().top + need > chunks_.back().cap) {
+        Chunk c;
+        c.cap = std::max<u64>(need, CHUNK_BYTES / 8);
+        c.top = 0;
+        if (!dev_alloc((void **)&c.base, c.cap * 8, s)) return nullptr;
+        chunks_.push_back(c);
+    }
+    Chunk &c = chunks_.back();
+    u64 *p = c.base + c.top;
+    c.blocks.push_back({p, need, true});
+    c.top += need;
+    return p;
+}
+
+void LayerStore::release(const u64 *p, cudaStream_t s)
+{
+    for (auto &c : chunks_)
+        for (auto &b : c.blocks)
+            if (b.p == p) b.live = false;
+    // pop released blocks from the top, and empty chunks
+    while (!chunks_.empty()) {
+        Chunk &c = chunks_.back();
+        while (!c.blocks.empty() && !c.blocks.back().live) {
+            c.top -= c.blocks.back().n;
+            c.blocks.pop_back();
+        }
+        if (!c.blocks.empty()) break;
+        dev_free(c.base, s);
+        chunks_.pop_back();
+    }
+}
+
+void LayerStore::clear(cudaStream_t s)
+{
+    for (auto &c : chunks_) dev_free(c.base, s);
+    chunks_.clear();
+}
+
+u64 LayerStore::bytes_in_use() const
+{
+    u64 b = 0;
+    for (auto &c : chunks_) b += c.top * 8;
+    return b;
 }
 
 // ---- engine -----------------------------------------------------------------
@@ -81,7 +197,9 @@ bool Engine::init(int dev)
     if (!io_stream && !CGB_CUDA(cudaStreamCreateWithFlags(&io_stream, cudaStreamNonBlocking))) return false;
     cudaMemPool_t pool;
     if (!CGB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev))) return false;
-    u64 keep = ~0ull;  // keep freed blocks cached in the pool between layers
+    // keep freed blocks cached in the pool between layer steps; an allocation
+    // that fails returns the cache to the device and retries (dev_alloc)
+    u64 keep = ~0ull;
     if (!CGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep))) return false;
     if (!ctr.d) {
         void *p;

@@ -117,4 +117,21 @@ void drop(DevBuf<T> &b, cudaStream_t s)
     b.n = b.cap = 0;
 }
 
+// Resident layers of a sweep.  Layers are appended during generation and
+// released top-down during the solve (last in, first out), so they are packed
+// into a few large chunks instead of one allocation per layer; nothing is
+// fragmented by the short-lived working buffers of each layer step.
+class LayerStore {
+  public:
+    static constexpr u64 CHUNK_BYTES = 4ull << 30;
+    u64 *push(u64 n, cudaStream_t s);       // room for n boards (nullptr on failure)
+    void release(const u64 *p, cudaStream_t s);  // frees a pushed block (LIFO fast path)
+    void clear(cudaStream_t s);
+    u64 bytes_in_use() const;
+  private:
+    struct Block { u64 *p; u64 n; bool live; };
+    struct Chunk { u64 *base; u64 cap; u64 top; std::vector<Block> blocks; };
+    std::vector<Chunk> chunks_;
+};
+
 }  // namespace cgb

@@ -224,9 +224,13 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
     const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
+    kclock().begin(s, &kstats().expand_ms);
     expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err);
+    kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_word(n_out, c.d, s)) return false;
+    kclock().flush();
+    kstats().expand_bytes += 8 * (n + *n_out);
     return check(c, s, "expand_moves");
 }
 
@@ -236,9 +240,14 @@ bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s)
     if (n == 0) return true;
     if (!CGB_CUDA(cudaMemsetAsync(c.d + 1, 0, sizeof(u64), s))) return false;
     const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
+    kclock().begin(s, &kstats().spawn_ms);
     count_spawns_kernel<<<grid, 256, 0, s>>>(in, n, c.d + 1);
+    kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    return read_word(total, c.d + 1, s);
+    if (!read_word(total, c.d + 1, s)) return false;
+    kclock().flush();
+    kstats().spawn_bytes += 8 * n;
+    return true;
 }
 
 bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c, cudaStream_t s)
@@ -248,9 +257,13 @@ bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_o
     if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
     const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
+    kclock().begin(s, &kstats().spawn_ms);
     expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err);
+    kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_word(n_out, c.d, s)) return false;
+    kclock().flush();
+    kstats().spawn_bytes += 8 * n + 16 * *n_out;
     return check(c, s, "expand_spawns");
 }
 

@@ -59,7 +59,7 @@ __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
 
 // best of the four moves of b, successors looked up canonicalised
 template <typename V>
-__device__ __forceinline__ V best_move(const RowTable &rt, u64 b, const DevTable<V> &t)
+__device__ __forceinline__ V best_move(const RowTable &rt, u64 b, const DevTable<V> &t, u32 &probes)
 {
     u64 v[4];
     views(b, v);
@@ -67,9 +67,17 @@ __device__ __forceinline__ V best_move(const RowTable &rt, u64 b, const DevTable
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         u64 m;
-        p[k] = move_left(rt, v[k], &m) == 2 ? table_lookup(t, canonical(m)) : V(0);
+        const bool legal = move_left(rt, v[k], &m) == 2;
+        probes += legal;
+        p[k] = legal ? table_lookup(t, canonical(m)) : V(0);
     }
     return vmax(vmax(p[0], p[1]), vmax(p[2], p[3]));
+}
+
+__device__ __forceinline__ void add_probes(u32 probes, u64 *counter)
+{
+    const u32 w = __reduce_add_sync(0xffffffffu, probes);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd((unsigned long long *)counter, (unsigned long long)w);
 }
 
 __device__ __forceinline__ bool satisfied(u64 b, const SolveRules &r)
@@ -92,11 +100,12 @@ __device__ __forceinline__ void stage_table_s(unsigned char *smem, const unsigne
 __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f64_kernel(const u64 *__restrict__ keys, u64 n,
                                                                      double *__restrict__ out, DevTable<double> t2,
                                                                      DevTable<double> t4, SolveRules r,
-                                                                     const unsigned short *g_move)
+                                                                     const unsigned short *g_move, u64 *probes_out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
     const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    u32 probes = 0;
     for (u64 i = (u64)blockIdx.x * SOLVE_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * SOLVE_THREADS) {
         const u64 b = keys[i];
         double res;
@@ -109,8 +118,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f64_kernel(const u64 *
             while (e) {  // cells in order 0..15 = highest nibble first
                 const int bit = 63 - __clzll(e);
                 e &= ~(1ull << bit);
-                s2 = __dadd_rn(s2, best_move(rt, b | (1ull << bit), t2));
-                s4 = __dadd_rn(s4, best_move(rt, b | (2ull << bit), t4));
+                s2 = __dadd_rn(s2, best_move(rt, b | (1ull << bit), t2, probes));
+                s4 = __dadd_rn(s4, best_move(rt, b | (2ull << bit), t4, probes));
             }
             res = 0.0;
             if (spaces) {
@@ -121,16 +130,18 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f64_kernel(const u64 *
         }
         out[i] = res;
     }
+    add_probes(probes, probes_out);
 }
 
 __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f32_kernel(const u64 *__restrict__ keys, u64 n,
                                                                      float *__restrict__ out, DevTable<float> t2,
                                                                      DevTable<float> t4, SolveRules r,
-                                                                     const unsigned short *g_move)
+                                                                     const unsigned short *g_move, u64 *probes_out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
     const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    u32 probes = 0;
     for (u64 i = (u64)blockIdx.x * SOLVE_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * SOLVE_THREADS) {
         const u64 b = keys[i];
         float res;
@@ -143,11 +154,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f32_kernel(const u64 *
             while (e) {
                 const int bit = 63 - __clzll(e);
                 e &= ~(1ull << bit);
-                const float y2 = __fsub_rn(best_move(rt, b | (1ull << bit), t2), c2);
+                const float y2 = __fsub_rn(best_move(rt, b | (1ull << bit), t2, probes), c2);
                 const float u2 = __fadd_rn(s2, y2);
                 c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
                 s2 = u2;
-                const float y4 = __fsub_rn(best_move(rt, b | (2ull << bit), t4), c4);
+                const float y4 = __fsub_rn(best_move(rt, b | (2ull << bit), t4, probes), c4);
                 const float u4 = __fadd_rn(s4, y4);
                 c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
                 s4 = u4;
@@ -163,6 +174,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f32_kernel(const u64 *
         }
         out[i] = res;
     }
+    add_probes(probes, probes_out);
 }
 
 // ---- bucket offsets --------------------------------------------------------
@@ -233,6 +245,28 @@ static int solve_grid(u64 n)
     return (int)std::max<u64>(1, std::min<u64>(need, (u64)sms));
 }
 
+template <typename K, typename V>
+static bool launch_solve(K kernel, const u64 *keys, u64 n, V *out, DevTable<V> t2, DevTable<V> t4,
+                         const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s, int vbytes)
+{
+    if (!CGB_CUDA(cudaMemsetAsync(c.d + 2, 0, sizeof(u64), s))) return false;
+    kclock().begin(s, &kstats().solve_ms);
+    kernel<<<solve_grid(n), SOLVE_THREADS, TABLE_BYTES_S, s>>>(keys, n, out, t2, t4, r, rt.move, c.d + 2);
+    kclock().end(s);
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    u64 probes = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(&probes, c.d + 2, sizeof(u64), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    kclock().flush();
+    KernelStats &k = kstats();
+    k.solve_launches++;
+    k.solve_boards += n;
+    k.lookups += probes;
+    // keys in, values out, one key sector and one value sector per probe
+    k.solve_bytes += (8 + vbytes) * n + 64 * probes;
+    return true;
+}
+
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
                      const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
 {
@@ -244,9 +278,8 @@ bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, 
             return false;
         attr = true;
     }
-    solve_f64_kernel<<<solve_grid(n), SOLVE_THREADS, TABLE_BYTES_S, s>>>(keys, n, out, dev_table<double>(t2),
-                                                                         dev_table<double>(t4), r, rt.move);
-    return CGB_CUDA(cudaGetLastError());
+    return launch_solve(solve_f64_kernel, keys, n, out, dev_table<double>(t2), dev_table<double>(t4), r, rt, c, s,
+                        8);
 }
 
 bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, const LayerIndex &t4,
@@ -260,9 +293,8 @@ bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, c
             return false;
         attr = true;
     }
-    solve_f32_kernel<<<solve_grid(n), SOLVE_THREADS, TABLE_BYTES_S, s>>>(keys, n, out, dev_table<float>(t2),
-                                                                         dev_table<float>(t4), r, rt.move);
-    return CGB_CUDA(cudaGetLastError());
+    return launch_solve(solve_f32_kernel, keys, n, out, dev_table<float>(t2), dev_table<float>(t4), r, rt, c, s,
+                        4);
 }
 
 }  // namespace cgb

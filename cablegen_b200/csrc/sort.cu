@@ -447,7 +447,10 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     if (!ws.reserve(n, s)) return false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (W_COUNT + 1) * sizeof(u32), s))) return false;
     const int hist_blocks = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
+    kclock().begin(s, &kstats().hist_ms);
     digit_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, n, ws.small + W_HIST);
+    kclock().end(s);
+    kstats().hist_bytes += 8 * n;
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u32 hist[8 * RADIX];
     if (!CGB_CUDA(cudaMemcpyAsync(hist, ws.small + W_HIST, sizeof(hist), cudaMemcpyDeviceToHost, s))) return false;
@@ -459,8 +462,12 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     for (int p = 0; p < np; p++) {
         const int d = digits[p];
         if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * RADIX * sizeof(u32), s))) return false;
+        kclock().begin(s, &kstats().onesweep_ms);
         onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
                                                        ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);
+        kclock().end(s);
+        kstats().onesweep_bytes += 16 * n;
+        kstats().onesweep_launches++;
         if (!CGB_CUDA(cudaGetLastError())) return false;
         std::swap(src, dst);
     }
@@ -469,7 +476,9 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         stats->passes = np;
         stats->n = n;
     }
-    return check_err(ws, s, "sort_keys");
+    if (!check_err(ws, s, "sort_keys")) return false;
+    kclock().flush();
+    return true;
 }
 
 bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s)
@@ -484,12 +493,16 @@ bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, 
     const u32 tiles = ceil_div(n, UNQ_TILE);
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * sizeof(u32), s))) return false;
+    kclock().begin(s, &kstats().unique_ms);
     unique_kernel<<<tiles, UNQ_THREADS, 0, s>>>(in, (u32)n, out, ws.lookback, ws.small + W_CTR,
                                                 ws.small + W_COUNT, ws.small + W_ERR);
+    kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u32 cnt = 0;
     if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
     if (!check_err(ws, s, "unique_keys")) return false;
+    kclock().flush();
+    kstats().unique_bytes += 8 * (n + cnt);
     *n_out = cnt;
     return true;
 }
@@ -510,13 +523,18 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     u32 *splits = ws.lookback + ((u64)tiles + 1);
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, ((u64)tiles + 1) * sizeof(u32), s))) return false;
+    kclock().begin(s, &kstats().merge_ms);
     merge_partition_kernel<<<ceil_div(tiles + 1, 256), 256, 0, s>>>(a, (u32)na, b, (u32)nb, splits, tiles);
     merge_unique_kernel<<<tiles, MRG_THREADS, 0, s>>>(a, (u32)na, b, (u32)nb, splits, out, ws.lookback,
                                                       ws.small + W_CTR, ws.small + W_COUNT, ws.small + W_ERR);
+    kclock().end(s);
+    kstats().launches++;
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u32 cnt = 0;
     if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
     if (!check_err(ws, s, "merge_unique")) return false;
+    kclock().flush();
+    kstats().merge_bytes += 8 * (total + cnt);
     *n_out = cnt;
     return true;
 }

@@ -64,6 +64,38 @@ extern "C" {
 
 const char *cgb_last_error(void) { return last_error(); }
 
+int cgb_get_kernel_stats(cgb_kernel_stats *o)
+{
+    const KernelStats &k = kstats();
+    o->launches = k.launches;
+    o->hist_ms = k.hist_ms;
+    o->onesweep_ms = k.onesweep_ms;
+    o->unique_ms = k.unique_ms;
+    o->merge_ms = k.merge_ms;
+    o->expand_ms = k.expand_ms;
+    o->spawn_ms = k.spawn_ms;
+    o->solve_ms = k.solve_ms;
+    o->index_ms = k.index_ms;
+    o->hist_bytes = k.hist_bytes;
+    o->onesweep_bytes = k.onesweep_bytes;
+    o->unique_bytes = k.unique_bytes;
+    o->merge_bytes = k.merge_bytes;
+    o->expand_bytes = k.expand_bytes;
+    o->spawn_bytes = k.spawn_bytes;
+    o->solve_bytes = k.solve_bytes;
+    o->onesweep_launches = k.onesweep_launches;
+    o->solve_launches = k.solve_launches;
+    o->solve_boards = k.solve_boards;
+    o->lookups = k.lookups;
+    return 0;
+}
+
+int cgb_reset_kernel_stats(void)
+{
+    kstats() = KernelStats{};
+    return 0;
+}
+
 int cgb_init(int device)
 {
     CGB_TRY(E().init(device));
@@ -223,24 +255,29 @@ struct CopyOutSink : LayerSink {
 
 struct Layer {
     int sum;
-    DevBuf<u64> keys;
+    u64 *keys;
+    u64 n;
 };
 
 struct KeepSink : LayerSink {
     std::vector<Layer> layers;
+    LayerStore store;
     cgb_layer_fn fn = nullptr;
     void *user = nullptr;
     HostStage stage;
     u64 d2h = 0;
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
+        // the layer sits in a buffer sized for the raw move output (4x the
+        // input); keep an exact-size copy so resident layers cost 8 B/board
         Layer L;
         L.sum = sum;
-        L.keys.p = d;
-        L.keys.n = n;
-        L.keys.cap = n;
+        L.n = n;
+        L.keys = store.push(n, s);
+        if (!L.keys) return false;
+        if (n && !CGB_CUDA(cudaMemcpyAsync(L.keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
         layers.push_back(L);
-        *kept = true;
+        *kept = false;
         if (fn) {
             if (!stage.reserve(n * 8 + 8)) return false;
             if (n && !CGB_CUDA(cudaMemcpyAsync(stage.p, d, n * 8, cudaMemcpyDeviceToHost, s))) return false;
@@ -313,6 +350,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     sink.fn = layer_fn;
     sink.user = user;
     GenTimes tm;
+    const u64 launches0 = kstats().launches;
     cudaEvent_t ev[3];
     for (auto &x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], s);
@@ -347,8 +385,8 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         cur = Solved{};
         cur.sum = sum;
         if (it != by_sum.end()) {
-            cur.keys = sink.layers[it->second].keys.p;
-            cur.n = sink.layers[it->second].keys.n;
+            cur.keys = sink.layers[it->second].keys;
+            cur.n = sink.layers[it->second].n;
         }
         if (!dev_alloc(&cur.vals, cur.n * vbytes + 8, s)) {
             ok = false;
@@ -395,7 +433,10 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         if (t4.bucket) dev_free(t4.bucket, s);
         {
             auto it4 = by_sum.find(t4.sum);
-            if (t4.sum && it4 != by_sum.end()) drop(sink.layers[it4->second].keys, s);
+            if (t4.sum && it4 != by_sum.end() && sink.layers[it4->second].keys) {
+                sink.store.release(sink.layers[it4->second].keys, s);
+                sink.layers[it4->second].keys = nullptr;
+            }
         }
         t4 = t2;
         t2 = cur;
@@ -404,7 +445,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         if (x->vals) dev_free(x->vals, s);
         if (x->bucket) dev_free(x->bucket, s);
     }
-    for (auto &L : sink.layers) drop(L.keys, s);
+    sink.store.clear(s);
     dev_free(d_ws, s);
     cudaEventRecord(ev[2], s);
     cudaEventSynchronize(ev[2]);
@@ -414,6 +455,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     for (auto &x : ev) cudaEventDestroy(x);
     if (stats) {
         fill_gen_stats(stats, tm);
+        stats->gpu_launches = kstats().launches - launches0;
         stats->layers = sink.layers.size();
         stats->boards_solved = solved;
         stats->gen_ms = gen_ms;

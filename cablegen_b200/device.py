@@ -38,6 +38,16 @@ def set_rules(settings: Settings):
     check(lib().cgb_set_rules(C.byref(r)))
 
 
+def kernel_stats() -> dict:
+    k = _lib.KernelStats()
+    check(lib().cgb_get_kernel_stats(C.byref(k)))
+    return k.as_dict()
+
+
+def reset_kernel_stats():
+    check(lib().cgb_reset_kernel_stats())
+
+
 def to_device(a, device="cuda") -> torch.Tensor:
     a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
     return torch.from_numpy(a.view(np.int64)).to(device)

@@ -79,6 +79,21 @@ typedef struct {
     uint64_t gpu_launches;                     /* kernels launched by the library */
 } cgb_stats;
 
+/* Device time (ms, CUDA events around every launch) and algorithmic bytes per
+ * kernel family, accumulated since the last cgb_reset_kernel_stats().
+ * Algorithmic bytes: sort pass 16 B/key, histogram 8 B/key, unique 8 B per key
+ * in and out, merge 8 B per key in and out, move expansion 8 B in + 8 B per
+ * output, spawns 8 B in + 16 B per output pair, solve (8 + value) B/board +
+ * 64 B per table probe (one key sector + one value sector). */
+typedef struct {
+    uint64_t launches;
+    double hist_ms, onesweep_ms, unique_ms, merge_ms, expand_ms, spawn_ms, solve_ms, index_ms;
+    uint64_t hist_bytes, onesweep_bytes, unique_bytes, merge_bytes, expand_bytes, spawn_bytes, solve_bytes;
+    uint64_t onesweep_launches, solve_launches, solve_boards, lookups;
+} cgb_kernel_stats;
+int cgb_get_kernel_stats(cgb_kernel_stats *out);
+int cgb_reset_kernel_stats(void);
+
 /* Layer callback: the layer `sum` as a host array (valid during the call). */
 typedef int (*cgb_layer_fn)(void *user, int sum, const uint64_t *h_boards, uint64_t n);
 /* Table callback: keys and values (double, or float for precision 32). */
