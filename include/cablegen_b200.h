@@ -59,6 +59,20 @@ int cgb_merge_unique(const uint64_t *d_a, uint64_t na, const uint64_t *d_b, uint
 /* Canonical form of every board (canonicalize_b, src/board.c:314-337). */
 int cgb_canonicalize(const uint64_t *d_in, uint64_t n, uint64_t *d_out);
 
+/* Sort d_in[0,n) ascending and drop repeats into d_out (capacity n, must not
+ * alias d_in); *n_out = number of distinct keys.  No counterpart in the
+ * reference: this is cgb_sort + cgb_unique for callers that cannot let the
+ * library allocate device memory (a host whose caching allocator owns the
+ * GPU under a hard budget, or latency-sensitive code that cannot absorb
+ * cudaMalloc's device-wide synchronisation).  Its scratch is one fixed
+ * __device__ array (a little over 8 MiB, held by every GPU that loads the
+ * library until exit), so n is limited to 2^20 keys; larger n is rejected
+ * with an error.  The first call on a device looks up the array's address
+ * and should come before any stream capture.  Calls share the array: calls
+ * that overlap on the GPU race and must be serialised.  stream may be 0.
+ * Returns after the work on `stream` has finished. */
+int cgb_sort_unique_noalloc(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *n_out, void *stream);
+
 /* ---- solve of one layer (solve_layer, src/solve.c:289-340) ---------------
  * precision 64: d_out/d_v2/d_v4 are double; 32: float (Kahan sums).
  * (d_k2,d_v2,n2) and (d_k4,d_v4,n4): the s+2 and s+4 tables, keys sorted.
