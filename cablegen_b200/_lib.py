@@ -70,6 +70,8 @@ def _declare(L):
         "cgb_last_error": (C.c_char_p, []),
         "cgb_init": (C.c_int, [C.c_int]),
         "cgb_set_rules": (C.c_int, [C.POINTER(Rules)]),
+        "cgb_set_option": (C.c_int, [C.c_char_p, C.c_longlong]),
+        "cgb_get_option": (C.c_longlong, [C.c_char_p]),
         "cgb_expand_moves": (C.c_int, [vp, u64, vp, u64, pu64]),
         "cgb_count_spawns": (C.c_int, [vp, u64, pu64]),
         "cgb_expand_spawns": (C.c_int, [vp, u64, vp, vp, u64, pu64]),

@@ -54,6 +54,8 @@ struct Engine {
     SortWorkspace ws;
     Counters ctr;
     cgb_rules rules{};
+    int index_kind = INDEX_HASH;  // lookup structure of solved layers
+    int bucket_bits = 22;         // INDEX_BUCKET: bucket count = 2^bits
 
     static Engine &get();
     bool init(int dev);

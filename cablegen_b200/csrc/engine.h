@@ -67,20 +67,38 @@ struct SolveRules {
     int n_winstates = 0;
 };
 
-// lookup index over one solved layer: bucket offsets over the key bits that
-// follow the layer's common prefix
+// Lookup index over one solved layer (replaces the bisection of lookup(),
+// src/solve.c:108-164; every kind returns the value of the key or 0.0).
+enum IndexKind : int {
+    INDEX_BISECT = 0,  // bisection over the sorted keys (the reference's search)
+    INDEX_BUCKET = 1,  // top-bits bucket offsets after the common prefix, then bisection
+    INDEX_HASH = 2,    // open addressing, key and value in one 16-byte slot
+};
+
 struct LayerIndex {
+    int kind = INDEX_BISECT;
     const u64 *keys = nullptr;
     const void *vals = nullptr;   // double or float, aligned with keys
     u64 n = 0;
-    const u32 *bucket = nullptr;  // 2^bits + 1 offsets (null: plain bisection)
-    int shift = 0;                // bucket = (key << prefix) >> (64 - bits)
-    int prefix = 0;
+    // INDEX_BUCKET
+    const u32 *bucket = nullptr;  // 2^bits + 1 offsets
+    int prefix = 0;               // bucket = (key << prefix) >> (64 - bits)
     int bits = 0;
     u64 prefix_value = 0;         // the shared high bits (key >> (64 - prefix))
+    // INDEX_HASH
+    const void *slots = nullptr;  // cap slots of {u64 key, u64 value bits}; key 0 = empty
+    u64 cap = 0;
 };
 
-bool build_index(LayerIndex &ix, u32 **bucket_storage, u64 *bucket_capacity, int bits_hint, cudaStream_t s);
+// device storage owned by one index (reused across layers)
+struct IndexStorage {
+    void *p = nullptr;
+    u64 bytes = 0;
+};
+
+// builds ix (keys/vals/n already set) of the requested kind; vbytes = 8 or 4
+bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
+                 cudaStream_t s);
 
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
                      const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s);

@@ -9,36 +9,76 @@
 //     each successor looked up, canonicalised, in the s+2 / s+4 table; a miss
 //     is 0.0 (src/solve.c:108-164).  res = 0.9*S2/k + 0.1*S4/k.
 //
-// The FP64 kernel evaluates exactly the reference's operation sequence with
-// round-to-nearest intrinsics (no FMA contraction), so its values are
-// bit-identical.  The FP32 kernel keeps tables in FP32, accumulates the two
-// spawn sums with Kahan compensation, and forms the final weighted mean in
-// FP64 before rounding once to FP32 (a 0.9f weight would bias every layer by
-// 2.6e-8 relative).
+// The eight successor keys of one cell (2 spawns x 4 moves) are formed first
+// and their table probes issued together, so a thread keeps up to eight
+// independent loads in flight.
+//
+// FP64 evaluates exactly the reference's operation sequence with
+// round-to-nearest intrinsics (no FMA contraction): bit-identical values.
+// FP32 keeps table values in FP32, accumulates the two spawn sums with Kahan
+// compensation and forms the weighted mean in FP64 before rounding once (a
+// 0.9f weight alone would bias every layer by 2.6e-8 relative).
+//
+// Lookup structures (all exact; a miss returns 0 like the reference):
+//   INDEX_BISECT  branch-free bisection over the sorted layer
+//   INDEX_BUCKET  top bits after the layer's common prefix select a bucket of
+//                 the sorted layer, then bisection inside it
+//   INDEX_HASH    open addressing with linear probing; a 16-byte slot holds
+//                 the key and the value, so a hit costs one sector
 #include "engine.h"
 
 namespace cgb {
 
-constexpr int SOLVE_THREADS = 512;
+constexpr int SOLVE_THREADS = 1024;
 constexpr int TABLE_BYTES_S = 65536 * 2 + 2048 * 4;
 
 // ---- lookup ---------------------------------------------------------------
 template <typename V>
 struct DevTable {
+    int kind;
     const u64 *keys;
     const V *vals;
     u64 n;
-    const u32 *bucket;  // optional bucket offsets over the bits after the prefix
+    const u32 *bucket;
     int prefix, bits;
     u64 prefix_value;
+    const ulonglong2 *slots;
+    u64 cap;
 };
 
+// murmur3's 64-bit finaliser (public domain mixing function)
+__host__ __device__ __forceinline__ u64 mix64(u64 k)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+__device__ __forceinline__ u64 home_slot(u64 key, u64 cap) { return __umul64hi(mix64(key), cap); }
+
 template <typename V>
-__device__ __forceinline__ V table_lookup(const DevTable<V> &t, u64 key)
+__device__ __forceinline__ V from_bits(u64 b);
+template <>
+__device__ __forceinline__ double from_bits<double>(u64 b) { return __longlong_as_double((long long)b); }
+template <>
+__device__ __forceinline__ float from_bits<float>(u64 b) { return __uint_as_float((u32)b); }
+
+template <typename V>
+__device__ __forceinline__ u64 to_bits(V v);
+template <>
+__device__ __forceinline__ u64 to_bits<double>(double v) { return (u64)__double_as_longlong(v); }
+template <>
+__device__ __forceinline__ u64 to_bits<float>(float v) { return (u64)__float_as_uint(v); }
+
+template <typename V>
+__device__ __forceinline__ V sorted_lookup(const DevTable<V> &t, u64 key)
 {
     if (t.n == 0) return V(0);
     u64 lo = 0, len = t.n;
-    if (t.bucket) {
+    if (t.kind == INDEX_BUCKET) {
         if (t.prefix > 0 && (key >> (64 - t.prefix)) != t.prefix_value) return V(0);
         const u32 bk = (u32)((key << t.prefix) >> (64 - t.bits));
         const u32 b0 = __ldg(t.bucket + bk), b1 = __ldg(t.bucket + bk + 1);
@@ -54,24 +94,63 @@ __device__ __forceinline__ V table_lookup(const DevTable<V> &t, u64 key)
     return __ldg(t.keys + lo) == key ? __ldg(t.vals + lo) : V(0);
 }
 
-__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
-__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
-
-// best of the four moves of b, successors looked up canonicalised
+// continue a linear probe after the first slot missed
 template <typename V>
-__device__ __forceinline__ V best_move(const RowTable &rt, u64 b, const DevTable<V> &t, u32 &probes)
+__device__ __noinline__ V hash_probe_rest(const DevTable<V> &t, u64 key, u64 s)
+{
+    for (u64 i = 1; i < t.cap; i++) {
+        s = (s + 1 == t.cap) ? 0 : s + 1;
+        const ulonglong2 e = __ldg(t.slots + s);
+        if (e.x == key) return from_bits<V>(e.y);
+        if (e.x == 0) return V(0);
+    }
+    return V(0);
+}
+
+template <typename V>
+__device__ __forceinline__ V vmax(V a, V b) { return a > b ? a : b; }
+
+// values of the successors key[0..3] (legal[j] false -> 0) in table t
+template <typename V>
+__device__ __forceinline__ void lookup4(const DevTable<V> &t, const u64 *key, const bool *legal, V *out)
+{
+    if (t.kind == INDEX_HASH) {
+        if (t.cap == 0) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) out[j] = V(0);
+            return;
+        }
+        u64 s[4];
+        ulonglong2 e[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            s[j] = home_slot(key[j], t.cap);
+            e[j] = legal[j] ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (!legal[j] || e[j].x == 0) out[j] = V(0);
+            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
+            else out[j] = hash_probe_rest(t, key[j], s[j]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) out[j] = legal[j] ? sorted_lookup(t, key[j]) : V(0);
+    }
+}
+
+// the canonical successors of b after each of the four moves
+__device__ __forceinline__ void successors(const RowTable &rt, u64 b, u64 *key, bool *legal, u32 &probes)
 {
     u64 v[4];
     views(b, v);
-    V p[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         u64 m;
-        const bool legal = move_left(rt, v[k], &m) == 2;
-        probes += legal;
-        p[k] = legal ? table_lookup(t, canonical(m)) : V(0);
+        legal[k] = move_left(rt, v[k], &m) == 2;
+        key[k] = canonical(m);
+        probes += legal[k];
     }
-    return vmax(vmax(p[0], p[1]), vmax(p[2], p[3]));
 }
 
 __device__ __forceinline__ void add_probes(u32 probes, u64 *counter)
@@ -97,10 +176,11 @@ __device__ __forceinline__ void stage_table_s(unsigned char *smem, const unsigne
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f64_kernel(const u64 *__restrict__ keys, u64 n,
-                                                                     double *__restrict__ out, DevTable<double> t2,
-                                                                     DevTable<double> t4, SolveRules r,
-                                                                     const unsigned short *g_move, u64 *probes_out)
+template <typename V>
+__global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_kernel(const u64 *__restrict__ keys, u64 n,
+                                                                 V *__restrict__ out, DevTable<V> t2,
+                                                                 DevTable<V> t4, SolveRules r,
+                                                                 const unsigned short *g_move, u64 *probes_out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
@@ -108,60 +188,37 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f64_kernel(const u64 *
     u32 probes = 0;
     for (u64 i = (u64)blockIdx.x * SOLVE_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * SOLVE_THREADS) {
         const u64 b = keys[i];
-        double res;
+        V res;
         if (satisfied(b, r)) {
-            res = 1.0;
+            res = V(1);
         } else {
             u64 e = empty_mask(b);
             const int spaces = popc64(e);
-            double s2 = 0.0, s4 = 0.0;
+            // FP64: plain sums in cell order; FP32: Kahan-compensated sums
+            V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
             while (e) {  // cells in order 0..15 = highest nibble first
                 const int bit = 63 - __clzll(e);
                 e &= ~(1ull << bit);
-                s2 = __dadd_rn(s2, best_move(rt, b | (1ull << bit), t2, probes));
-                s4 = __dadd_rn(s4, best_move(rt, b | (2ull << bit), t4, probes));
-            }
-            res = 0.0;
-            if (spaces) {
-                const double k = (double)spaces;
-                res = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, s2), k), __ddiv_rn(__dmul_rn(0.1, s4), k));
-            }
-            if (r.score && res == 0.0) res = (double)tile_sum(b);
-        }
-        out[i] = res;
-    }
-    add_probes(probes, probes_out);
-}
-
-__global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f32_kernel(const u64 *__restrict__ keys, u64 n,
-                                                                     float *__restrict__ out, DevTable<float> t2,
-                                                                     DevTable<float> t4, SolveRules r,
-                                                                     const unsigned short *g_move, u64 *probes_out)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    stage_table_s(smem, g_move);
-    const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
-    u32 probes = 0;
-    for (u64 i = (u64)blockIdx.x * SOLVE_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * SOLVE_THREADS) {
-        const u64 b = keys[i];
-        float res;
-        if (satisfied(b, r)) {
-            res = 1.0f;
-        } else {
-            u64 e = empty_mask(b);
-            const int spaces = popc64(e);
-            float s2 = 0.f, c2 = 0.f, s4 = 0.f, c4 = 0.f;  // Kahan sums
-            while (e) {
-                const int bit = 63 - __clzll(e);
-                e &= ~(1ull << bit);
-                const float y2 = __fsub_rn(best_move(rt, b | (1ull << bit), t2, probes), c2);
-                const float u2 = __fadd_rn(s2, y2);
-                c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
-                s2 = u2;
-                const float y4 = __fsub_rn(best_move(rt, b | (2ull << bit), t4, probes), c4);
-                const float u4 = __fadd_rn(s4, y4);
-                c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
-                s4 = u4;
+                u64 k2[4], k4[4];
+                bool l2[4], l4[4];
+                successors(rt, b | (1ull << bit), k2, l2, probes);
+                successors(rt, b | (2ull << bit), k4, l4, probes);
+                V p2[4], p4[4];
+                lookup4(t2, k2, l2, p2);
+                lookup4(t4, k4, l4, p4);
+                const V best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
+                const V best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
+                if constexpr (sizeof(V) == 8) {
+                    s2 = __dadd_rn(s2, best2);
+                    s4 = __dadd_rn(s4, best4);
+                } else {
+                    const float y2 = __fsub_rn(best2, c2), u2 = __fadd_rn(s2, y2);
+                    c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
+                    s2 = u2;
+                    const float y4 = __fsub_rn(best4, c4), u4 = __fadd_rn(s4, y4);
+                    c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
+                    s4 = u4;
+                }
             }
             double d = 0.0;
             if (spaces) {
@@ -170,14 +227,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_f32_kernel(const u64 *
                 d = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, S2), k), __ddiv_rn(__dmul_rn(0.1, S4), k));
             }
             if (r.score && d == 0.0) d = (double)tile_sum(b);
-            res = (float)d;
+            res = (V)d;
         }
         out[i] = res;
     }
     add_probes(probes, probes_out);
 }
 
-// ---- bucket offsets --------------------------------------------------------
+// ---- index construction ----------------------------------------------------
 __global__ void bucket_offsets_kernel(const u64 *__restrict__ keys, u64 n, u32 *__restrict__ off, int prefix,
                                       int bits)
 {
@@ -190,31 +247,103 @@ __global__ void bucket_offsets_kernel(const u64 *__restrict__ keys, u64 n, u32 *
     }
 }
 
-bool build_index(LayerIndex &ix, u32 **storage, u64 *capacity, int bits_hint, cudaStream_t s)
+template <typename V>
+__global__ void hash_build_kernel(const u64 *__restrict__ keys, const V *__restrict__ vals, u64 n,
+                                  ulonglong2 *slots, u64 cap, u32 *err)
 {
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 key = keys[i];
+        u64 s = home_slot(key, cap);
+        bool placed = false;
+        for (u64 p = 0; p < cap; p++) {
+            const u64 prev = atomicCAS((unsigned long long *)&slots[s].x, 0ull, (unsigned long long)key);
+            if (prev == 0) {
+                slots[s].y = to_bits<V>(vals[i]);
+                placed = true;
+                break;
+            }
+            s = (s + 1 == cap) ? 0 : s + 1;
+        }
+        if (!placed) atomicOr(err, ERR_CAPACITY);
+    }
+}
+
+static int grid_for(u64 n, int threads, int per_sm)
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = NUM_SMS_B200;
+    const u64 need = (n + threads - 1) / threads;
+    return (int)std::max<u64>(1, std::min<u64>(need, (u64)sms * per_sm));
+}
+
+static bool ensure_storage(IndexStorage &st, u64 bytes, cudaStream_t s)
+{
+    if (st.bytes >= bytes && st.p) return true;
+    if (st.p) dev_free(st.p, s);
+    st.p = nullptr;
+    st.bytes = 0;
+    if (!dev_alloc(&st.p, bytes, s)) return false;
+    st.bytes = bytes;
+    return true;
+}
+
+bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
+                 cudaStream_t s)
+{
+    ix.kind = INDEX_BISECT;
     ix.bucket = nullptr;
-    ix.bits = 0;
-    if (ix.n < 64 || bits_hint <= 0) return true;
+    ix.slots = nullptr;
+    ix.cap = 0;
+    if (ix.n == 0 || kind == INDEX_BISECT) return true;
+    if (kind == INDEX_HASH) {
+        // load factor <= 0.45: capacity rounded up to a multiple of 64 slots
+        const u64 cap = ((ix.n * 20 / 9) + 63) / 64 * 64;
+        if (!ensure_storage(st, cap * 16, s)) return false;
+        if (!CGB_CUDA(cudaMemsetAsync(st.p, 0, cap * 16, s))) return false;
+        if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+        kclock().begin(s, &kstats().index_ms);
+        if (vbytes == 8)
+            hash_build_kernel<double><<<grid_for(ix.n, 256, 16), 256, 0, s>>>(
+                ix.keys, (const double *)ix.vals, ix.n, (ulonglong2 *)st.p, cap, c.err);
+        else
+            hash_build_kernel<float><<<grid_for(ix.n, 256, 16), 256, 0, s>>>(
+                ix.keys, (const float *)ix.vals, ix.n, (ulonglong2 *)st.p, cap, c.err);
+        kclock().end(s);
+        if (!CGB_CUDA(cudaGetLastError())) return false;
+        u32 e = 0;
+        if (!CGB_CUDA(cudaMemcpyAsync(&e, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+        if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+        kclock().flush();
+        if (e) {
+            set_error("build_index: device error " + err_string(e));
+            return false;
+        }
+        ix.kind = INDEX_HASH;
+        ix.slots = st.p;
+        ix.cap = cap;
+        return true;
+    }
+    // INDEX_BUCKET
+    if (ix.n < 64 || bucket_bits <= 0) return true;
     u64 first, last;
     if (!CGB_CUDA(cudaMemcpyAsync(&first, ix.keys, 8, cudaMemcpyDeviceToHost, s))) return false;
     if (!CGB_CUDA(cudaMemcpyAsync(&last, ix.keys + ix.n - 1, 8, cudaMemcpyDeviceToHost, s))) return false;
     if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     const u64 x = first ^ last;
     const int prefix = x ? __builtin_clzll(x) : 64;
-    int bits = bits_hint;
+    int bits = bucket_bits;
     if (bits > 64 - prefix) bits = 64 - prefix;
     if (bits <= 0) return true;
-    const u64 need = (1ull << bits) + 1;
-    if (*capacity < need) {
-        if (*storage) dev_free(*storage, s);
-        *storage = nullptr;
-        if (!dev_alloc((void **)storage, need * sizeof(u32), s)) return false;
-        *capacity = need;
-    }
-    const int grid = (int)std::min<u64>((ix.n + 256) / 256, (u64)NUM_SMS_B200 * 16);
-    bucket_offsets_kernel<<<grid, 256, 0, s>>>(ix.keys, ix.n, *storage, prefix, bits);
+    const u64 need = ((1ull << bits) + 1) * sizeof(u32);
+    if (!ensure_storage(st, need, s)) return false;
+    kclock().begin(s, &kstats().index_ms);
+    bucket_offsets_kernel<<<grid_for(ix.n + 1, 256, 16), 256, 0, s>>>(ix.keys, ix.n, (u32 *)st.p, prefix, bits);
+    kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    ix.bucket = *storage;
+    ix.kind = INDEX_BUCKET;
+    ix.bucket = (const u32 *)st.p;
     ix.prefix = prefix;
     ix.bits = bits;
     ix.prefix_value = prefix ? first >> (64 - prefix) : 0;
@@ -225,6 +354,7 @@ template <typename V>
 static DevTable<V> dev_table(const LayerIndex &ix)
 {
     DevTable<V> t;
+    t.kind = ix.kind;
     t.keys = ix.keys;
     t.vals = (const V *)ix.vals;
     t.n = ix.n;
@@ -232,26 +362,27 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     t.prefix = ix.prefix;
     t.bits = ix.bits;
     t.prefix_value = ix.prefix_value;
+    t.slots = (const ulonglong2 *)ix.slots;
+    t.cap = ix.kind == INDEX_HASH ? ix.cap : 0;
     return t;
 }
 
-static int solve_grid(u64 n)
+template <typename V>
+static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
+                         const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
 {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = NUM_SMS_B200;
-    const u64 need = (n + SOLVE_THREADS - 1) / SOLVE_THREADS;
-    return (int)std::max<u64>(1, std::min<u64>(need, (u64)sms));
-}
-
-template <typename K, typename V>
-static bool launch_solve(K kernel, const u64 *keys, u64 n, V *out, DevTable<V> t2, DevTable<V> t4,
-                         const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s, int vbytes)
-{
+    if (n == 0) return true;
+    static bool attr = false;
+    if (!attr) {
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           TABLE_BYTES_S)))
+            return false;
+        attr = true;
+    }
     if (!CGB_CUDA(cudaMemsetAsync(c.d + 2, 0, sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().solve_ms);
-    kernel<<<solve_grid(n), SOLVE_THREADS, TABLE_BYTES_S, s>>>(keys, n, out, t2, t4, r, rt.move, c.d + 2);
+    solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, TABLE_BYTES_S, s>>>(
+        keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u64 probes = 0;
@@ -263,38 +394,20 @@ static bool launch_solve(K kernel, const u64 *keys, u64 n, V *out, DevTable<V> t
     k.solve_boards += n;
     k.lookups += probes;
     // keys in, values out, one key sector and one value sector per probe
-    k.solve_bytes += (8 + vbytes) * n + 64 * probes;
+    k.solve_bytes += (8 + sizeof(V)) * n + 64 * probes;
     return true;
 }
 
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
                      const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
 {
-    if (n == 0) return true;
-    static bool attr = false;
-    if (!attr) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           TABLE_BYTES_S)))
-            return false;
-        attr = true;
-    }
-    return launch_solve(solve_f64_kernel, keys, n, out, dev_table<double>(t2), dev_table<double>(t4), r, rt, c, s,
-                        8);
+    return launch_solve<double>(keys, n, out, t2, t4, r, rt, c, s);
 }
 
 bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, const LayerIndex &t4,
                      const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
 {
-    if (n == 0) return true;
-    static bool attr = false;
-    if (!attr) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           TABLE_BYTES_S)))
-            return false;
-        attr = true;
-    }
-    return launch_solve(solve_f32_kernel, keys, n, out, dev_table<float>(t2), dev_table<float>(t4), r, rt, c, s,
-                        4);
+    return launch_solve<float>(keys, n, out, t2, t4, r, rt, c, s);
 }
 
 }  // namespace cgb

@@ -96,6 +96,36 @@ int cgb_reset_kernel_stats(void)
     return 0;
 }
 
+int cgb_set_option(const char *name, long long value)
+{
+    const std::string k = name ? name : "";
+    if (k == "index") {
+        if (value < INDEX_BISECT || value > INDEX_HASH) {
+            set_error("cgb_set_option: index must be 0 (bisect), 1 (bucket) or 2 (hash)");
+            return -1;
+        }
+        E().index_kind = (int)value;
+    } else if (k == "bucket_bits") {
+        if (value < 0 || value > 30) {
+            set_error("cgb_set_option: bucket_bits must be in 0..30");
+            return -1;
+        }
+        E().bucket_bits = (int)value;
+    } else {
+        set_error("cgb_set_option: unknown option " + k);
+        return -1;
+    }
+    return 0;
+}
+
+long long cgb_get_option(const char *name)
+{
+    const std::string k = name ? name : "";
+    if (k == "index") return E().index_kind;
+    if (k == "bucket_bits") return E().bucket_bits;
+    return -1;
+}
+
 int cgb_init(int device)
 {
     CGB_TRY(E().init(device));
@@ -216,13 +246,20 @@ extern "C" int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, 
     t4.keys = d_k4;
     t4.vals = d_v4;
     t4.n = n4;
+    const int vb = precision == 32 ? 4 : 8;
+    IndexStorage st2, st4;
+    bool ok = build_index(t2, E().index_kind, vb, st2, E().bucket_bits, E().ctr, s) &&
+              build_index(t4, E().index_kind, vb, st4, E().bucket_bits, E().ctr, s);
     const SolveRules r = make_solve_rules(E().rules, d_ws, (int)ws.size());
-    bool ok;
-    if (precision == 32)
-        ok = solve_layer_f32(d_keys, n, (float *)d_out, t2, t4, r, E().rt, E().ctr, s);
-    else
-        ok = solve_layer_f64(d_keys, n, (double *)d_out, t2, t4, r, E().rt, E().ctr, s);
+    if (ok) {
+        if (precision == 32)
+            ok = solve_layer_f32(d_keys, n, (float *)d_out, t2, t4, r, E().rt, E().ctr, s);
+        else
+            ok = solve_layer_f64(d_keys, n, (double *)d_out, t2, t4, r, E().rt, E().ctr, s);
+    }
     dev_free(d_ws, s);
+    dev_free(st2.p, s);
+    dev_free(st4.p, s);
     CGB_TRY(ok);
     CGB_TRY(E().sync());
     return 0;
@@ -368,8 +405,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         const u64 *keys = nullptr;
         void *vals = nullptr;
         u64 n = 0;
-        u32 *bucket = nullptr;
-        u64 bucket_cap = 0;
+        IndexStorage store;
         LayerIndex ix;
     };
     Solved t2, t4, cur;
@@ -426,11 +462,11 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         cur.ix.n = cur.n;
         {
             Timer t(s, &index_ms);
-            ok = build_index(cur.ix, &cur.bucket, &cur.bucket_cap, 0, s);
+            ok = build_index(cur.ix, e.index_kind, vbytes, cur.store, e.bucket_bits, e.ctr, s);
         }
         // the s+4 table is no longer needed: free its values, bucket and keys
         if (t4.vals) dev_free(t4.vals, s);
-        if (t4.bucket) dev_free(t4.bucket, s);
+        if (t4.store.p) dev_free(t4.store.p, s);
         {
             auto it4 = by_sum.find(t4.sum);
             if (t4.sum && it4 != by_sum.end() && sink.layers[it4->second].keys) {
@@ -443,7 +479,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     }
     for (Solved *x : {&t2, &t4}) {
         if (x->vals) dev_free(x->vals, s);
-        if (x->bucket) dev_free(x->bucket, s);
+        if (x->store.p) dev_free(x->store.p, s);
     }
     sink.store.clear(s);
     dev_free(d_ws, s);

@@ -38,6 +38,14 @@ def set_rules(settings: Settings):
     check(lib().cgb_set_rules(C.byref(r)))
 
 
+def set_option(name: str, value: int):
+    check(lib().cgb_set_option(name.encode(), int(value)))
+
+
+def get_option(name: str) -> int:
+    return int(lib().cgb_get_option(name.encode()))
+
+
 def kernel_stats() -> dict:
     k = _lib.KernelStats()
     check(lib().cgb_get_kernel_stats(C.byref(k)))

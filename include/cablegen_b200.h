@@ -35,6 +35,12 @@ int cgb_init(int device);
 const char *cgb_last_error(void);
 /* Build and upload the row table for these rules (generate_lut, src/board.c:100-132). */
 int cgb_set_rules(const cgb_rules *rules);
+/* Tuning knobs: "index" = lookup structure of solved layers (0 bisection of the
+ * sorted layer as in lookup(), src/solve.c:108-164; 1 top-bits buckets then
+ * bisection; 2 open-addressing hash, the default), "bucket_bits" (buckets of
+ * kind 1).  cgb_get_option returns -1 for an unknown name. */
+int cgb_set_option(const char *name, long long value);
+long long cgb_get_option(const char *name);
 
 /* ---- device primitives of one layer step --------------------------------
  * Move + prune + canonicalise every board (the move workers,

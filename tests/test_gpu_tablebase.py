@@ -23,8 +23,20 @@ def test_generate_matches_reference(cuda, name):
     assert st["boards_generated"] == sum(r["boards"] for r in d.values())
 
 
+INDEX_KINDS = [0, 1, 2]  # bisection, top-bits buckets, hash
+
+
+@pytest.fixture
+def index_kind(cuda, request):
+    old = cuda.get_option("index")
+    cuda.set_option("index", request.param)
+    yield request.param
+    cuda.set_option("index", old)
+
+
+@pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
 @pytest.mark.parametrize("name", ["plain_2x4", "plain_2x4_nearwall"])
-def test_tablebase_fp64_bit_exact(cuda, name):
+def test_tablebase_fp64_bit_exact(cuda, name, index_kind):
     w = configs.get(name)
     f = w.formations[0]
     cuda.set_rules(w.settings)
@@ -38,7 +50,8 @@ def test_tablebase_fp64_bit_exact(cuda, name):
     assert all(len(tables[s][0]) == 0 for s in tables if s < f.start)
 
 
-def test_tablebase_fp32_error(cuda):
+@pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
+def test_tablebase_fp32_error(cuda, index_kind):
     w = configs.get("plain_2x4_nearwall")
     f = w.formations[0]
     cuda.set_rules(w.settings)
@@ -48,7 +61,8 @@ def test_tablebase_fp32_error(cuda):
     assert err <= 1e-6, err
 
 
-def test_solve_layer_matches_oracle(cuda):
+@pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
+def test_solve_layer_matches_oracle(cuda, index_kind):
     """One layer through cgb_solve_layer against the oracle, with nox and score variants."""
     w = configs.get("plain_2x4_nearwall")
     f = w.formations[0]
