@@ -46,43 +46,89 @@ inline u32 prmt(u32 a, u32 sel)
 __host__ __device__ __forceinline__ u32 rev_rows32(u32 x)
 {
     x = prmt(x, 0x2301);                                      // swap bytes inside each half-word
-    return ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4); // swap nibbles inside each byte
+    return ((x >> 4) & 0x0F0F0F0Fu) | ((x << 4) & 0xF0F0F0F0u); // swap nibbles inside each byte
 }
+
+// A board as two 32-bit words: hi = rows 0-1 (cells 0..7), lo = rows 2-3.
+struct Half {
+    u32 hi, lo;
+};
+__host__ __device__ __forceinline__ Half halves(u64 b) { return Half{(u32)(b >> 32), (u32)b}; }
+__host__ __device__ __forceinline__ u64 whole(Half h) { return make64(h.hi, h.lo); }
 
 // V: reverse the order of the four rows
-__host__ __device__ __forceinline__ u64 flip_v(u64 b)
-{
-    u32 hi = (u32)(b >> 32), lo = (u32)b;
-    return make64(prmt(lo, 0x1032), prmt(hi, 0x1032));
-}
-
+__host__ __device__ __forceinline__ Half flip_v(Half b) { return Half{prmt(b.lo, 0x1032), prmt(b.hi, 0x1032)}; }
 // H: mirror every row left<->right
-__host__ __device__ __forceinline__ u64 flip_h(u64 b)
+__host__ __device__ __forceinline__ Half flip_h(Half b) { return Half{rev_rows32(b.hi), rev_rows32(b.lo)}; }
+// T: transpose the 4x4 nibble matrix (cell (r,c) <-> (c,r)): inside each
+// 2x2 block by one delta swap per word (cells 1<->4, 3<->6, 9<->12, 11<->14),
+// then the off-diagonal 2x2 blocks by two byte permutes across the words
+// (cells 2,3 <-> 8,9 and 6,7 <-> 12,13).
+__host__ __device__ __forceinline__ Half transpose(Half b)
 {
-    return make64(rev_rows32((u32)(b >> 32)), rev_rows32((u32)b));
+    u32 t = ((b.hi >> 12) ^ b.hi) & 0x0000F0F0u;
+    const u32 hi = b.hi ^ t ^ (t << 12);
+    t = ((b.lo >> 12) ^ b.lo) & 0x0000F0F0u;
+    const u32 lo = b.lo ^ t ^ (t << 12);
+#ifdef __CUDA_ARCH__
+    return Half{__byte_perm(hi, lo, 0x3715), __byte_perm(hi, lo, 0x2604)};
+#else
+    auto perm2 = [](u32 x, u32 y, u32 sel) {
+        const u64 v = ((u64)y << 32) | x;
+        u32 out = 0;
+        for (int i = 0; i < 4; i++) out |= (u32)((v >> (8 * ((sel >> (4 * i)) & 7))) & 0xFF) << (8 * i);
+        return out;
+    };
+    return Half{perm2(hi, lo, 0x3715), perm2(hi, lo, 0x2604)};
+#endif
 }
 
-// T: transpose the 4x4 nibble matrix (cell (r,c) <-> (c,r)) by two delta swaps:
-// inside every 2x2 block, then the two off-diagonal 2x2 blocks.
-__host__ __device__ __forceinline__ u64 transpose(u64 b)
-{
-    u64 t = ((b >> 12) ^ b) & 0x0000F0F00000F0F0ull;   // cells 4,6,12,14 <-> 1,3,9,11
-    b ^= t ^ (t << 12);
-    t = ((b >> 24) ^ b) & 0x00000000FF00FF00ull;       // cells 8,9,12,13 <-> 2,3,6,7
-    b ^= t ^ (t << 24);
-    return b;
-}
+__host__ __device__ __forceinline__ u64 flip_v(u64 b) { return whole(flip_v(halves(b))); }
+__host__ __device__ __forceinline__ u64 flip_h(u64 b) { return whole(flip_h(halves(b))); }
+__host__ __device__ __forceinline__ u64 transpose(u64 b) { return whole(transpose(halves(b))); }
 
 __host__ __device__ __forceinline__ u64 umax64(u64 a, u64 b) { return a > b ? a : b; }
+
+// the 8 images of the square's symmetry group: {X, X.T} for X in {id, V, H, VH}
+__host__ __device__ __forceinline__ void images(u64 b, u64 img[8])
+{
+    const Half h = halves(b), t = transpose(h);
+    const Half hv = flip_v(h), tv = flip_v(t), hh = flip_h(h), th = flip_h(t);
+    img[0] = whole(h);
+    img[1] = whole(hv);
+    img[2] = whole(hh);
+    img[3] = whole(flip_v(hh));
+    img[4] = whole(t);
+    img[5] = whole(tv);
+    img[6] = whole(th);
+    img[7] = whole(flip_v(th));
+}
 
 // canonical representative: unsigned max over the 8 symmetries
 __host__ __device__ __forceinline__ u64 canonical(u64 b)
 {
-    u64 t = transpose(b);
-    u64 bv = flip_v(b), tv = flip_v(t);
-    u64 m0 = umax64(b, bv), m1 = umax64(flip_h(b), flip_h(bv));
-    u64 m2 = umax64(t, tv), m3 = umax64(flip_h(t), flip_h(tv));
-    return umax64(umax64(m0, m1), umax64(m2, m3));
+    u64 im[8];
+    images(b, im);
+    return umax64(umax64(umax64(im[0], im[1]), umax64(im[2], im[3])),
+                  umax64(umax64(im[4], im[5]), umax64(im[6], im[7])));
+}
+
+// Cell permutations of the images: image k of (b with cell c set) equals
+// image k of b with cell image_cell(k, c) set.  Cell c = 4r + q.
+//   V: (r,q)->(3-r,q)  H: (r,q)->(r,3-q)  T: (r,q)->(q,r)
+__host__ __device__ __forceinline__ int image_cell(int k, int c)
+{
+    const int r = c >> 2, q = c & 3;
+    switch (k) {
+    case 0: return c;                          // id
+    case 1: return 4 * (3 - r) + q;            // V
+    case 2: return 4 * r + (3 - q);            // H
+    case 3: return 4 * (3 - r) + (3 - q);      // VH
+    case 4: return 4 * q + r;                  // T
+    case 5: return 4 * (3 - q) + r;            // V.T
+    case 6: return 4 * q + (3 - r);            // H.T
+    default: return 4 * (3 - q) + (3 - r);     // VH.T
+    }
 }
 
 // reference rotate_clockwise (src/board.c:239-248): new (r,c) = old (3-c, r)
@@ -198,12 +244,19 @@ __device__ __forceinline__ int move_left(const RowTable &t, u64 y, u64 *out)
 }
 
 // the four move views of b: {b, H b, T b, H T b} for left, right, up, down
-__device__ __forceinline__ void views(u64 b, u64 v[4])
+__host__ __device__ __forceinline__ void views(u64 b, u64 v[4])
 {
+    const Half h = halves(b), t = transpose(h);
     v[0] = b;
-    v[1] = flip_h(b);
-    v[2] = transpose(b);
-    v[3] = flip_h(v[2]);
+    v[1] = whole(flip_h(h));
+    v[2] = whole(t);
+    v[3] = whole(flip_h(t));
+}
+
+// cell of view k (id, H, T, H.T) that holds cell c of the board
+__host__ __device__ __forceinline__ int view_cell(int k, int c)
+{
+    return image_cell(k == 0 ? 0 : k == 1 ? 2 : k == 2 ? 4 : 6, c);
 }
 
 }  // namespace cgb

@@ -46,6 +46,15 @@ struct LayerSink {
     virtual bool layer(int sum, u64 *d_boards, u64 n, cudaStream_t s, bool *kept) = 0;
 };
 
+// working buffers of the generation sweep, kept between layers and calls
+struct GenBuffers {
+    DevBuf<u64> a, b;          // raw move output and its sort scratch
+    DevBuf<u64> c[3];          // raw spawn streams and their sort scratch
+    DevBuf<u64> S;             // boards of the next layer to move
+    DevBuf<u64> u2, u4, u4_next;
+    DevBuf<u64> moved;         // the current layer
+};
+
 struct Engine {
     int device = -1;
     bool ready = false;
@@ -63,9 +72,11 @@ struct Engine {
     PruneParams prune_params() const;
     bool sync();
 
-    bool move_layer(const u64 *d_in, u64 n, DevBuf<u64> &moved, GenTimes *tm);
-    bool spawn_layer(const u64 *d_moved, u64 n, DevBuf<u64> &u2, DevBuf<u64> &u4, GenTimes *tm);
+    GenBuffers gen;
+    bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
+    bool spawn_layer(GenTimes *tm);
     bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm);
+    void release_buffers();
 };
 
 }  // namespace cgb

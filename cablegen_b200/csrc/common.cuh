@@ -76,6 +76,17 @@ __device__ __forceinline__ void st_release(u32 *p, u32 v)
 {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+// relaxed (non-caching) accesses: enough when the word carries its own flag
+__device__ __forceinline__ u32 ld_relaxed(const u32 *p)
+{
+    u32 v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(u32 *p, u32 v)
+{
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ __forceinline__ u64 ld_acquire64(const u64 *p)
 {
     u64 v;

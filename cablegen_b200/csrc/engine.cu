@@ -230,133 +230,121 @@ PruneParams Engine::prune_params() const
 
 bool Engine::sync() { return CGB_CUDA(cudaStreamSynchronize(stream)); }
 
+// grow-only device buffer with 25 % headroom, so layer after layer of slowly
+// growing sizes reuses the same allocation
+static bool reserve(DevBuf<u64> &b, u64 n, cudaStream_t s)
+{
+    if (b.p && b.cap >= n) return true;
+    return grow(b, n + n / 4 + 1024, s);
+}
+
 // moved = unique(sort(expand_moves(S)))
-bool Engine::move_layer(const u64 *d_in, u64 n, DevBuf<u64> &moved, GenTimes *tm)
+bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
 {
     cudaStream_t s = stream;
-    DevBuf<u64> a, b;
+    GenBuffers &g = gen;
     const u64 cap = 4 * n;
-    if (!grow(a, cap, s) || !grow(b, cap, s)) return false;
+    if (!reserve(g.a, cap, s) || !reserve(g.b, cap, s)) return false;
     u64 nr = 0;
-    {
-        Timer t(s, tm ? &tm->expand_ms : nullptr);
-        if (!expand_moves(d_in, n, a.p, cap, &nr, rt, prune_params(), ctr, s)) return false;
-    }
-    u64 *sorted = a.p;
+    if (!expand_moves(d_in, n, g.a.p, cap, &nr, rt, prune_params(), ctr, s)) return false;
+    u64 *sorted = g.a.p;
     SortStats st;
-    {
-        Timer t(s, tm ? &tm->sort_ms : nullptr);
-        if (!sort_keys(a.p, b.p, nr, &sorted, ws, s, &st)) return false;
-    }
+    if (!sort_keys(g.a.p, g.b.p, nr, &sorted, ws, s, &st)) return false;
     if (tm) {
         tm->sorted_keys += nr;
         tm->sort_passes += (u64)st.passes * nr;
     }
-    // unique from the sorted buffer into the other one
-    DevBuf<u64> src = (sorted == a.p) ? a : b;
-    DevBuf<u64> dst = (sorted == a.p) ? b : a;
+    DevBuf<u64> &full = (sorted == g.a.p) ? g.a : g.b;
+    DevBuf<u64> &free_ = (sorted == g.a.p) ? g.b : g.a;
     u64 nm = 0;
-    {
-        Timer t(s, tm ? &tm->unique_ms : nullptr);
-        if (!unique_keys(src.p, nr, dst.p, &nm, ws, s)) return false;
-    }
-    drop(src, s);
-    drop(moved, s);
-    moved = dst;
-    moved.n = nm;
+    if (!unique_keys(full.p, nr, free_.p, &nm, ws, s)) return false;
+    std::swap(free_, g.moved);   // the layer; the old layer buffer becomes scratch
+    g.moved.n = nm;
     return true;
 }
 
-// U2 / U4: sorted unique canonical 2-spawns and 4-spawns of the moved layer
-bool Engine::spawn_layer(const u64 *d_moved, u64 n, DevBuf<u64> &u2, DevBuf<u64> &u4, GenTimes *tm)
+// U2 / U4: sorted unique canonical 2-spawns and 4-spawns of the moved layer;
+// U2 lands in g.u2, U4 in g.u4_next
+bool Engine::spawn_layer(GenTimes *tm)
 {
     cudaStream_t s = stream;
+    GenBuffers &g = gen;
+    const u64 *d_moved = g.moved.p;
+    const u64 n = g.moved.n;
     u64 total = 0;
     if (!count_spawns(d_moved, n, &total, ctr, s)) return false;
-    DevBuf<u64> x2, x4, spare;
-    if (!grow(x2, total, s) || !grow(x4, total, s) || !grow(spare, total, s)) return false;
+    for (auto &x : g.c)
+        if (!reserve(x, total, s)) return false;
     u64 ns = 0;
-    {
-        Timer t(s, tm ? &tm->expand_ms : nullptr);
-        if (!expand_spawns(d_moved, n, x2.p, x4.p, total, &ns, ctr, s)) return false;
-    }
-    DevBuf<u64> *outs[2] = {&u2, &u4};
-    DevBuf<u64> ins[2] = {x2, x4};
+    if (!expand_spawns(d_moved, n, g.c[0].p, g.c[1].p, total, &ns, ctr, s)) return false;
+    // round 1 sorts c[0] with c[2] as scratch; round 2 sorts c[1] with the
+    // buffer that round 1 left free
+    int in_idx[2] = {0, 1};
+    int spare = 2;
+    int out_idx[2];
     for (int k = 0; k < 2; k++) {
-        DevBuf<u64> in = ins[k];
+        DevBuf<u64> &in = g.c[in_idx[k]];
         u64 *sorted = in.p;
         SortStats st;
-        {
-            Timer t(s, tm ? &tm->sort_ms : nullptr);
-            if (!sort_keys(in.p, spare.p, ns, &sorted, ws, s, &st)) return false;
-        }
+        if (!sort_keys(in.p, g.c[spare].p, ns, &sorted, ws, s, &st)) return false;
         if (tm) {
             tm->sorted_keys += ns;
             tm->sort_passes += (u64)st.passes * ns;
         }
-        DevBuf<u64> full = (sorted == in.p) ? in : spare;   // holds the sorted keys
-        DevBuf<u64> free_ = (sorted == in.p) ? spare : in;  // receives the unique keys
+        const int full = (sorted == in.p) ? in_idx[k] : spare;
+        const int dst = (sorted == in.p) ? spare : in_idx[k];
         u64 nu = 0;
-        {
-            Timer t(s, tm ? &tm->unique_ms : nullptr);
-            if (!unique_keys(full.p, ns, free_.p, &nu, ws, s)) return false;
-        }
-        drop(*outs[k], s);
-        *outs[k] = free_;
-        outs[k]->n = nu;
-        spare = full;  // its contents are no longer needed
+        if (!unique_keys(g.c[full].p, ns, g.c[dst].p, &nu, ws, s)) return false;
+        g.c[dst].n = nu;
+        out_idx[k] = dst;
+        spare = full;
     }
-    drop(spare, s);
+    std::swap(g.u2, g.c[out_idx[0]]);
+    std::swap(g.u4_next, g.c[out_idx[1]]);
     return true;
 }
 
 bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm)
 {
     cudaStream_t s = stream;
-    DevBuf<u64> S, U4, moved, U2, next;
-    if (!grow(S, n_init, s)) return false;
-    if (n_init && !CGB_CUDA(cudaMemcpyAsync(S.p, h_initial, n_init * 8, cudaMemcpyHostToDevice, s))) return false;
-    S.n = n_init;
+    GenBuffers &g = gen;
+    if (!reserve(g.S, n_init, s)) return false;
+    if (n_init && !CGB_CUDA(cudaMemcpyAsync(g.S.p, h_initial, n_init * 8, cudaMemcpyHostToDevice, s))) return false;
+    g.S.n = n_init;
+    g.u4.n = 0;
     bool ok = true;
     for (int layer = start; layer <= end && ok; layer += 2) {
-        ok = move_layer(S.p, S.n, moved, tm);
+        ok = move_layer(g.S.p, g.S.n, tm);
         if (!ok) break;
-        drop(S, s);
-        ok = spawn_layer(moved.p, moved.n, U2, next, tm);
+        ok = spawn_layer(tm);
         if (!ok) break;
         // S_{s+2} = U2 u U4(previous layer)
-        if (!grow(S, U2.n + U4.n, s)) {
+        if (!reserve(g.S, g.u2.n + g.u4.n, s)) {
             ok = false;
             break;
         }
         u64 nm = 0;
-        {
-            Timer t(s, tm ? &tm->merge_ms : nullptr);
-            ok = merge_unique(U2.p, U2.n, U4.p, U4.n, S.p, &nm, ws, s);
-        }
+        ok = merge_unique(g.u2.p, g.u2.n, g.u4.p, g.u4.n, g.S.p, &nm, ws, s);
         if (!ok) break;
-        S.n = nm;
-        drop(U2, s);
-        drop(U4, s);
-        U4 = next;
-        next.p = nullptr;
-        next.cap = next.n = 0;
-        if (tm) tm->boards += moved.n;
-        // hand the layer to the sink (it may keep the buffer)
+        g.S.n = nm;
+        std::swap(g.u4, g.u4_next);
+        if (tm) tm->boards += g.moved.n;
         bool kept = false;
-        ok = sink.layer(layer, moved.p, moved.n, s, &kept);
+        ok = sink.layer(layer, g.moved.p, g.moved.n, s, &kept);
         if (kept) {
-            moved.p = nullptr;
-            moved.cap = moved.n = 0;
+            g.moved.p = nullptr;
+            g.moved.cap = g.moved.n = 0;
         }
     }
-    drop(S, s);
-    drop(U4, s);
-    drop(U2, s);
-    drop(moved, s);
-    drop(next, s);
     if (ok) ok = sync();
     return ok;
+}
+
+void Engine::release_buffers()
+{
+    GenBuffers &g = gen;
+    for (DevBuf<u64> *b : {&g.a, &g.b, &g.c[0], &g.c[1], &g.c[2], &g.S, &g.u2, &g.u4, &g.u4_next, &g.moved})
+        drop(*b, stream);
 }
 
 }  // namespace cgb

@@ -15,6 +15,7 @@ struct SortWorkspace {
     u32 *small = nullptr;       // histograms, tile counters, error word, counts
     u32 *lookback = nullptr;    // decoupled look-back state
     u64 lookback_bytes = 0;
+    bool err_dirty = false;     // a sort left its errors in the word for unique to report
     bool reserve(u64 n, cudaStream_t s);
     void release(cudaStream_t s);
 };
@@ -28,6 +29,8 @@ int sort_plan(const u32 *hist_host, u64 n, int *digits);
 // sorts keys[0,n) ascending using tmp[0,n); *sorted points at keys or tmp
 bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cudaStream_t s,
                SortStats *stats = nullptr);
+// reports device errors a sort left behind (when no unique_keys follows)
+bool sort_check(SortWorkspace &ws, cudaStream_t s);
 // out must not alias in
 bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s);
 // sorted union of two sorted duplicate-free runs, without repeats

@@ -17,7 +17,7 @@
 
 namespace cgb {
 
-constexpr int EXP_THREADS = 512;
+constexpr int EXP_THREADS = 1024;
 constexpr int TABLE_BYTES = 65536 * 2 + 2048 * 4;
 
 void build_row_table(int free_formation, int ignore_f, unsigned short *move, u32 *ok)
@@ -167,11 +167,22 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
         if (pos + cnt > cap) {
             if (cnt) atomicOr(err, ERR_CAPACITY);
         } else {
+            // the images of b once; a spawn adds one nibble to each image
+            u64 im[8];
+            images(b, im);
             while (e) {
                 const int bit = 63 - __clzll(e);  // nibble's low bit
                 e &= ~(1ull << bit);
-                out2[pos] = canonical(b | (1ull << bit));
-                out4[pos] = canonical(b | (2ull << bit));
+                const int cell = (60 - bit) >> 2;
+                u64 m2 = 0, m4 = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int sh = 60 - 4 * image_cell(k, cell);
+                    m2 = umax64(m2, im[k] | (1ull << sh));
+                    m4 = umax64(m4, im[k] | (2ull << sh));
+                }
+                out2[pos] = m2;
+                out4[pos] = m4;
                 pos++;
             }
         }
@@ -194,6 +205,22 @@ static bool read_word(u64 *dst, const u64 *src, cudaStream_t s)
 {
     if (!CGB_CUDA(cudaMemcpyAsync(dst, src, sizeof(u64), cudaMemcpyDeviceToHost, s))) return false;
     return CGB_CUDA(cudaStreamSynchronize(s));
+}
+
+// one copy for a count word and the error word (Counters keeps the error word
+// 32 words after the counts)
+static bool read_count_checked(u64 *dst, Counters &c, int idx, cudaStream_t s, const char *what)
+{
+    u64 words[33];
+    if (!CGB_CUDA(cudaMemcpyAsync(words, c.d, sizeof words, cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
+    const u32 e = (u32)words[32];
+    if (e) {
+        set_error(std::string(what) + ": device error " + err_string(e));
+        return false;
+    }
+    *dst = words[idx];
+    return true;
 }
 
 static bool check(Counters &c, cudaStream_t s, const char *what)
@@ -228,10 +255,10 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    if (!read_word(n_out, c.d, s)) return false;
+    if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;
     kclock().flush();
     kstats().expand_bytes += 8 * (n + *n_out);
-    return check(c, s, "expand_moves");
+    return true;
 }
 
 bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s)
@@ -261,10 +288,10 @@ bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_o
     expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    if (!read_word(n_out, c.d, s)) return false;
+    if (!read_count_checked(n_out, c, 0, s, "expand_spawns")) return false;
     kclock().flush();
     kstats().spawn_bytes += 8 * n + 16 * *n_out;
-    return check(c, s, "expand_spawns");
+    return true;
 }
 
 }  // namespace cgb

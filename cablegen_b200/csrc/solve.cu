@@ -9,9 +9,8 @@
 //     each successor looked up, canonicalised, in the s+2 / s+4 table; a miss
 //     is 0.0 (src/solve.c:108-164).  res = 0.9*S2/k + 0.1*S4/k.
 //
-// The eight successor keys of one cell (2 spawns x 4 moves) are formed first
-// and their table probes issued together, so a thread keeps up to eight
-// independent loads in flight.
+// Work is compacted per warp: only legal moves are canonicalised and probed
+// (see solve_kernel).
 //
 // FP64 evaluates exactly the reference's operation sequence with
 // round-to-nearest intrinsics (no FMA contraction): bit-identical values.
@@ -29,7 +28,8 @@
 
 namespace cgb {
 
-constexpr int SOLVE_THREADS = 1024;
+constexpr int SOLVE_THREADS = 512;
+constexpr int SOLVE_SMEM = 65536 * 2 + 2048 * 4 + (512 / 32) * 2 * 128 * 8 * 2;
 constexpr int TABLE_BYTES_S = 65536 * 2 + 2048 * 4;
 
 // ---- lookup ---------------------------------------------------------------
@@ -46,18 +46,20 @@ struct DevTable {
     u64 cap;
 };
 
-// murmur3's 64-bit finaliser (public domain mixing function)
-__host__ __device__ __forceinline__ u64 mix64(u64 k)
+// 32-bit hash of a board: both halves multiplied by odd constants, then
+// xor-shift / multiply rounds (constants of the murmur3 and xxhash32
+// finalisers); range-reduced by a multiply-high, so tables need not be a
+// power of two (capacity < 2^32 slots).
+__host__ __device__ __forceinline__ u32 hash32(u64 k)
 {
-    k ^= k >> 33;
-    k *= 0xff51afd7ed558ccdull;
-    k ^= k >> 33;
-    k *= 0xc4ceb9fe1a85ec53ull;
-    k ^= k >> 33;
-    return k;
+    u32 x = ((u32)(k >> 32) * 0x9E3779B1u) ^ ((u32)k * 0x85EBCA77u);
+    x ^= x >> 15;
+    x *= 0xC2B2AE3Du;
+    x ^= x >> 13;
+    return x;
 }
 
-__device__ __forceinline__ u64 home_slot(u64 key, u64 cap) { return __umul64hi(mix64(key), cap); }
+__device__ __forceinline__ u64 home_slot(u64 key, u64 cap) { return __umulhi(hash32(key), (u32)cap); }
 
 template <typename V>
 __device__ __forceinline__ V from_bits(u64 b);
@@ -110,47 +112,18 @@ __device__ __noinline__ V hash_probe_rest(const DevTable<V> &t, u64 key, u64 s)
 template <typename V>
 __device__ __forceinline__ V vmax(V a, V b) { return a > b ? a : b; }
 
-// values of the successors key[0..3] (legal[j] false -> 0) in table t
 template <typename V>
-__device__ __forceinline__ void lookup4(const DevTable<V> &t, const u64 *key, const bool *legal, V *out)
+__device__ __forceinline__ V table_value(const DevTable<V> &t, u64 key)
 {
     if (t.kind == INDEX_HASH) {
-        if (t.cap == 0) {
-#pragma unroll
-            for (int j = 0; j < 4; j++) out[j] = V(0);
-            return;
-        }
-        u64 s[4];
-        ulonglong2 e[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            s[j] = home_slot(key[j], t.cap);
-            e[j] = legal[j] ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (!legal[j] || e[j].x == 0) out[j] = V(0);
-            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
-            else out[j] = hash_probe_rest(t, key[j], s[j]);
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) out[j] = legal[j] ? sorted_lookup(t, key[j]) : V(0);
+        if (t.cap == 0) return V(0);
+        const u64 s = home_slot(key, t.cap);
+        const ulonglong2 e = __ldg(t.slots + s);
+        if (e.x == key) return from_bits<V>(e.y);
+        if (e.x == 0) return V(0);
+        return hash_probe_rest(t, key, s);
     }
-}
-
-// the canonical successors of b after each of the four moves
-__device__ __forceinline__ void successors(const RowTable &rt, u64 b, u64 *key, bool *legal, u32 &probes)
-{
-    u64 v[4];
-    views(b, v);
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        u64 m;
-        legal[k] = move_left(rt, v[k], &m) == 2;
-        key[k] = canonical(m);
-        probes += legal[k];
-    }
+    return sorted_lookup(t, key);
 }
 
 __device__ __forceinline__ void add_probes(u32 probes, u64 *counter)
@@ -176,6 +149,15 @@ __device__ __forceinline__ void stage_table_s(unsigned char *smem, const unsigne
     __syncthreads();
 }
 
+// Each warp solves 32 boards at a time.  Every round takes the next empty
+// cell of each lane's board, forms the (up to) 8 moved successors of the two
+// spawns from the board's four move views (computed once per board), and
+// appends the legal ones to a per-warp queue in shared memory.  The warp then
+// canonicalises and looks up the queued boards 32 at a time -- only legal
+// moves cost a canonical form and a probe -- and each lane folds its best
+// values into its sums in cell order.
+constexpr int SOLVE_Q = 128;  // queue entries per spawn per warp (32 lanes x 4 moves)
+
 template <typename V>
 __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_kernel(const u64 *__restrict__ keys, u64 n,
                                                                  V *__restrict__ out, DevTable<V> t2,
@@ -185,8 +167,159 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_kernel(const u64 *__re
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
     const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    u64 *qk = (u64 *)(smem + TABLE_BYTES_S) + (u64)warp * (2 * SOLVE_Q);                     // [2][Q] boards
+    V *qv = (V *)(smem + TABLE_BYTES_S + (SOLVE_THREADS / 32) * 2 * SOLVE_Q * 8) + warp * (2 * SOLVE_Q);
     u32 probes = 0;
-    for (u64 i = (u64)blockIdx.x * SOLVE_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * SOLVE_THREADS) {
+    const u64 stride = (u64)gridDim.x * SOLVE_THREADS;
+    for (u64 base = (u64)blockIdx.x * SOLVE_THREADS + warp * 32; base < n; base += stride) {
+        const u64 i = base + lane;
+        const bool active = i < n;
+        const u64 b = active ? keys[i] : 0;
+        const bool sat = active && satisfied(b, r);
+        u64 e = (active && !sat) ? empty_mask(b) : 0;
+        const int spaces = popc64(e);
+        u64 v[4];
+        views(b, v);
+        V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
+        while (__any_sync(0xffffffffu, e != 0)) {
+            u64 m2[4], m4[4];
+            u32 l2 = 0, l4 = 0;
+            const bool has = e != 0;
+            if (has) {
+                const int bit = 63 - __clzll(e);
+                e &= ~(1ull << bit);
+                const int cell = (60 - bit) >> 2;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int sh = 60 - 4 * view_cell(k, cell);
+                    if (move_left(rt, v[k] | (1ull << sh), &m2[k]) == 2) l2 |= 1u << k;
+                    if (move_left(rt, v[k] | (2ull << sh), &m4[k]) == 2) l4 |= 1u << k;
+                }
+                probes += __popc(l2) + __popc(l4);
+            }
+            // append the legal successors to the warp's queues
+            const u32 n2 = __popc(l2), n4 = __popc(l4);
+            const u32 packed = n2 | (n4 << 16);
+            const u32 inc = warp_inclusive_scan(packed);
+            const u32 tot = __shfl_sync(0xffffffffu, inc, 31);
+            const u32 off2 = (inc - packed) & 0xFFFF, off4 = (inc - packed) >> 16;
+            const u32 tot2 = tot & 0xFFFF, tot4 = tot >> 16;
+            {
+                u32 j2 = off2, j4 = off4;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (l2 & (1u << k)) qk[j2++] = m2[k];
+                    if (l4 & (1u << k)) qk[SOLVE_Q + j4++] = m4[k];
+                }
+            }
+            __syncwarp();
+            const u32 tmax = tot2 > tot4 ? tot2 : tot4;
+            for (u32 q = lane; q < tmax; q += 32) {
+                const bool do2 = q < tot2, do4 = q < tot4;
+                const u64 k2 = do2 ? canonical(qk[q]) : 0;
+                const u64 k4 = do4 ? canonical(qk[SOLVE_Q + q]) : 0;
+                if (t2.kind == INDEX_HASH && t4.kind == INDEX_HASH) {
+                    // issue both first probes before resolving either
+                    const u64 sa = (do2 && t2.cap) ? home_slot(k2, t2.cap) : 0;
+                    const u64 sb = (do4 && t4.cap) ? home_slot(k4, t4.cap) : 0;
+                    const ulonglong2 ea = (do2 && t2.cap) ? __ldg(t2.slots + sa) : make_ulonglong2(0, 0);
+                    const ulonglong2 eb = (do4 && t4.cap) ? __ldg(t4.slots + sb) : make_ulonglong2(0, 0);
+                    if (do2)
+                        qv[q] = (ea.x == k2) ? from_bits<V>(ea.y) : (ea.x == 0 ? V(0) : hash_probe_rest(t2, k2, sa));
+                    if (do4)
+                        qv[SOLVE_Q + q] =
+                            (eb.x == k4) ? from_bits<V>(eb.y) : (eb.x == 0 ? V(0) : hash_probe_rest(t4, k4, sb));
+                } else {
+                    if (do2) qv[q] = table_value(t2, k2);
+                    if (do4) qv[SOLVE_Q + q] = table_value(t4, k4);
+                }
+            }
+            __syncwarp();
+            if (has) {
+                V best2 = 0, best4 = 0;
+                u32 j2 = off2, j4 = off4;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (l2 & (1u << k)) best2 = vmax(best2, qv[j2++]);
+                    if (l4 & (1u << k)) best4 = vmax(best4, qv[SOLVE_Q + j4++]);
+                }
+                if constexpr (sizeof(V) == 8) {  // cell order, plain IEEE adds
+                    s2 = __dadd_rn(s2, best2);
+                    s4 = __dadd_rn(s4, best4);
+                } else {  // Kahan-compensated
+                    const float y2 = __fsub_rn(best2, c2), u2 = __fadd_rn(s2, y2);
+                    c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
+                    s2 = u2;
+                    const float y4 = __fsub_rn(best4, c4), u4 = __fadd_rn(s4, y4);
+                    c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
+                    s4 = u4;
+                }
+            }
+            __syncwarp();
+        }
+        if (active) {
+            V res;
+            if (sat) {
+                res = V(1);
+            } else {
+                double d = 0.0;
+                if (spaces) {
+                    const double k = (double)spaces;
+                    const double S2 = (double)s2 - (double)c2, S4 = (double)s4 - (double)c4;
+                    d = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, S2), k), __ddiv_rn(__dmul_rn(0.1, S4), k));
+                }
+                if (r.score && d == 0.0) d = (double)tile_sum(b);
+                res = (V)d;
+            }
+            out[i] = res;
+        }
+    }
+    add_probes(probes, probes_out);
+}
+
+// Direct variant: one thread per board, no queue.  The eight successors of
+// one cell (2 spawns x 4 moves) are formed from the board's four views (the
+// spawned nibble is OR-ed into each view), canonicalised and probed together,
+// so a thread keeps up to eight independent loads in flight.
+constexpr int DIRECT_THREADS = 1024;
+
+template <typename V>
+__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out)
+{
+    if (t.kind == INDEX_HASH) {
+        u64 s[4];
+        ulonglong2 e[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && t.cap;
+            s[j] = on ? home_slot(key[j], t.cap) : 0;
+            e[j] = on ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (!((legal >> j) & 1) || e[j].x == 0) out[j] = V(0);
+            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
+            else out[j] = hash_probe_rest(t, key[j], s[j]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) out[j] = ((legal >> j) & 1) ? sorted_lookup(t, key[j]) : V(0);
+    }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u64 *__restrict__ keys, u64 n,
+                                                                         V *__restrict__ out, DevTable<V> t2,
+                                                                         DevTable<V> t4, SolveRules r,
+                                                                         const unsigned short *g_move,
+                                                                         u64 *probes_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    stage_table_s(smem, g_move);
+    const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    u32 probes = 0;
+    for (u64 i = (u64)blockIdx.x * DIRECT_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * DIRECT_THREADS) {
         const u64 b = keys[i];
         V res;
         if (satisfied(b, r)) {
@@ -194,18 +327,28 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_kernel(const u64 *__re
         } else {
             u64 e = empty_mask(b);
             const int spaces = popc64(e);
-            // FP64: plain sums in cell order; FP32: Kahan-compensated sums
+            u64 v[4];
+            views(b, v);
             V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
             while (e) {  // cells in order 0..15 = highest nibble first
                 const int bit = 63 - __clzll(e);
                 e &= ~(1ull << bit);
+                const int cell = (60 - bit) >> 2;
                 u64 k2[4], k4[4];
-                bool l2[4], l4[4];
-                successors(rt, b | (1ull << bit), k2, l2, probes);
-                successors(rt, b | (2ull << bit), k4, l4, probes);
+                u32 l2 = 0, l4 = 0;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int sh = 60 - 4 * view_cell(k, cell);
+                    u64 m;
+                    if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
+                    k2[k] = canonical(m);
+                    if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
+                    k4[k] = canonical(m);
+                }
+                probes += __popc(l2) + __popc(l4);
                 V p2[4], p4[4];
-                lookup4(t2, k2, l2, p2);
-                lookup4(t4, k4, l4, p4);
+                probe4(t2, k2, l2, p2);
+                probe4(t4, k4, l4, p4);
                 const V best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
                 const V best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
                 if constexpr (sizeof(V) == 8) {
@@ -367,6 +510,8 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     return t;
 }
 
+int g_solve_variant = 0;  // 0: direct (one thread per board), 1: warp-compacted queue
+
 template <typename V>
 static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
                          const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
@@ -375,14 +520,21 @@ static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, c
     static bool attr = false;
     if (!attr) {
         if (!CGB_CUDA(cudaFuncSetAttribute(solve_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           SOLVE_SMEM)))
+            return false;
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            TABLE_BYTES_S)))
             return false;
         attr = true;
     }
     if (!CGB_CUDA(cudaMemsetAsync(c.d + 2, 0, sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().solve_ms);
-    solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, TABLE_BYTES_S, s>>>(
-        keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
+    if (g_solve_variant == 1)
+        solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, SOLVE_SMEM, s>>>(
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
+    else
+        solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u64 probes = 0;

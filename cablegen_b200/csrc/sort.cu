@@ -36,6 +36,60 @@ constexpr int MRG_THREADS = 256;
 constexpr int MRG_KPT = 8;
 constexpr int MRG_TILE = MRG_THREADS * MRG_KPT;
 
+// Walk back over the look-back words of one bin (or of the whole tile),
+// LB_BATCH predecessors per round trip, polling with a short sleep while a
+// predecessor has not published.  Each word carries its own flag, so relaxed
+// accesses suffice.  Returns the sum of the predecessors' counts up to and
+// including the first inclusive prefix.
+#ifndef LB_BATCH
+#define LB_BATCH 4
+#endif
+__device__ __forceinline__ u32 lookback_sum(const u32 *words, u64 stride, int j, u32 *err)
+{
+    u32 excl = 0;
+    u32 spins = 0;
+    while (j >= 0) {
+        u32 v[LB_BATCH];
+#pragma unroll
+        for (int q = 0; q < LB_BATCH; q++) v[q] = (j - q >= 0) ? ld_relaxed(words + (u64)(j - q) * stride) : LB_PRE;
+        bool done = false, stalled = false;
+#pragma unroll
+        for (int q = 0; q < LB_BATCH; q++) {
+            if (done || stalled) continue;
+            const u32 flag = v[q] & ~LB_MASK;
+            if (flag == 0) {
+                stalled = true;  // not published yet: poll again from here
+            } else {
+                excl += v[q] & LB_MASK;
+                if (flag == LB_PRE) done = true;
+                else j--;
+            }
+        }
+        if (done) break;
+        if (stalled) {
+            if (++spins > SPIN_LIMIT) {
+                atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    return excl;
+}
+
+// decoupled look-back over one u32 count per tile; returns the exclusive prefix
+__device__ __forceinline__ u32 tile_lookback(u32 *lookback, u32 tile, u32 count, u32 *err)
+{
+    if (tile == 0) {
+        st_relaxed(lookback, LB_PRE | count);
+        return 0;
+    }
+    st_relaxed(lookback + tile, LB_AGG | count);
+    const u32 excl = lookback_sum(lookback, 1, (int)tile - 1, err);
+    st_relaxed(lookback + tile, LB_PRE | (excl + count));
+    return excl;
+}
+
 // ---------------------------------------------------------------------------
 // histogram of all eight byte digits in one pass
 __global__ void __launch_bounds__(256) digit_histogram_kernel(const u64 *__restrict__ keys, u64 n,
@@ -131,26 +185,11 @@ __global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__res
     u32 *lb = lookback + (u64)tile * RADIX + d;
     u32 excl = 0;
     if (tile == 0) {
-        st_release(lb, LB_PRE | cnt);
+        st_relaxed(lb, LB_PRE | cnt);
     } else {
-        st_release(lb, LB_AGG | cnt);
-        int j = (int)tile - 1;
-        u32 spins = 0;
-        while (j >= 0) {
-            const u32 v = ld_acquire(lookback + (u64)j * RADIX + d);
-            const u32 flag = v & ~LB_MASK;
-            if (flag == 0) {
-                if (++spins > SPIN_LIMIT) {
-                    atomicOr(err, ERR_LOOKBACK_TIMEOUT);
-                    break;
-                }
-                continue;
-            }
-            excl += v & LB_MASK;
-            if (flag == LB_PRE) break;
-            j--;
-        }
-        st_release(lb, LB_PRE | (excl + cnt));
+        st_relaxed(lb, LB_AGG | cnt);
+        excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
+        st_relaxed(lb, LB_PRE | (excl + cnt));
     }
     u32 total;
     const u32 gexcl = block_exclusive_scan<u32>(digit_hist[d], scan_scratch, &total);
@@ -179,35 +218,117 @@ __global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__res
 }
 
 // ---------------------------------------------------------------------------
-// decoupled look-back over one u32 count per tile; returns the exclusive prefix
-__device__ __forceinline__ u32 tile_lookback(u32 *lookback, u32 tile, u32 count, u32 *err)
+// Second form of the digit pass: lanes find their equal-digit peers with eight
+// ballots (one per digit bit) instead of a match instruction, ranks are packed
+// two per register so four CTAs fit per SM, and the tile is scattered into
+// shared memory before the look-back so that wait overlaps useful work.
+// Walk back over the per-tile look-back words of one bin, eight predecessors
+// per round trip: the eight loads are independent, so a long walk costs one
+// latency per eight tiles instead of one per tile.  Returns the sum of the
+// predecessors' counts up to and including the first inclusive prefix.
+constexpr int BAL_KPT = 16;
+constexpr int BAL_TILE = SORT_THREADS * BAL_KPT;  // 4096 keys per tile
+
+__global__ void __launch_bounds__(SORT_THREADS, 5)
+    onesweep_ballot_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
+                           const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err)
 {
-    u32 excl = 0;
-    if (tile == 0) {
-        st_release(lookback, LB_PRE | count);
-        return 0;
+    __shared__ u64 keys_sh[BAL_TILE];
+    __shared__ u32 warp_hist[SORT_THREADS / 32][RADIX];
+    __shared__ u32 bin_local[RADIX];
+    __shared__ u32 bin_global[RADIX];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u32 tile_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < (SORT_THREADS / 32) * RADIX; i += SORT_THREADS) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const u32 tile = tile_sh;
+    const u32 tile_base = tile * BAL_TILE;
+    const u32 warp_base = tile_base + warp * (BAL_KPT * 32);
+
+    // only the digits stay in registers (four per word); the keys are read
+    // again for the local scatter, from L2
+    u32 dg[BAL_KPT / 4];
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        const u32 dd = idx < n ? (u32)(src[idx] >> shift) & 0xFF : 0;
+        if (i % 4 == 0) dg[i / 4] = dd;
+        else dg[i / 4] |= dd << (8 * (i % 4));
     }
-    st_release(lookback + tile, LB_AGG | count);
-    int j = (int)tile - 1;
-    u32 spins = 0;
-    while (j >= 0) {
-        const u32 v = ld_acquire(lookback + j);
-        const u32 flag = v & ~LB_MASK;
-        if (flag == 0) {
-            if (++spins > SPIN_LIMIT) {
-                atomicOr(err, ERR_LOOKBACK_TIMEOUT);
-                break;
-            }
-            continue;
+    const u32 lt = lanemask_lt();
+    u32 rank2[BAL_KPT / 2];
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        const u32 valid = __ballot_sync(0xffffffffu, idx < n);
+        const u32 d = (dg[i / 4] >> (8 * (i % 4))) & 0xFF;
+        u32 peers = valid;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const u32 bj = __ballot_sync(0xffffffffu, (d >> j) & 1);
+            peers &= ((d >> j) & 1) ? bj : ~bj;
         }
-        excl += v & LB_MASK;
-        if (flag == LB_PRE) break;
-        j--;
+        const u32 base = warp_hist[warp][d];   // every peer reads the same word
+        __syncwarp();
+        if (idx < n && (peers & lt) == 0) warp_hist[warp][d] = base + __popc(peers);
+        __syncwarp();
+        const u32 r = base + __popc(peers & lt);
+        if (i & 1) rank2[i >> 1] |= r << 16;
+        else rank2[i >> 1] = r;
     }
-    st_release(lookback + tile, LB_PRE | (excl + count));
-    return excl;
+    __syncthreads();
+
+    // per bin: warp offsets inside the tile, tile count; publish the aggregate
+    const u32 d = threadIdx.x;  // SORT_THREADS == RADIX
+    u32 cnt = 0;
+#pragma unroll
+    for (int w = 0; w < SORT_THREADS / 32; w++) {
+        const u32 c = warp_hist[w][d];
+        warp_hist[w][d] = cnt;
+        cnt += c;
+    }
+    u32 *lb = lookback + (u64)tile * RADIX + d;
+    st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
+    u32 total;
+    const u32 lstart = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
+    bin_local[d] = lstart;
+    __syncthreads();
+    // local scatter: the tile sorted by this digit, in shared memory
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        if (idx < n) {
+            const u64 key = src[idx];
+            const u32 dd = (dg[i / 4] >> (8 * (i % 4))) & 0xFF;
+            const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xFFFF;
+            keys_sh[bin_local[dd] + warp_hist[warp][dd] + r] = key;
+        }
+    }
+    // look-back for this bin's global offset
+    u32 excl = 0;
+    if (tile != 0) {
+        excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
+        st_relaxed(lb, LB_PRE | (excl + cnt));
+    }
+    const u32 gexcl = block_exclusive_scan<u32>(digit_hist[d], scan_scratch, &total);
+    bin_global[d] = gexcl + excl;
+    __syncthreads();
+    const u32 tile_n = min((u32)BAL_TILE, n - tile_base);
+    for (u32 j = threadIdx.x; j < tile_n; j += SORT_THREADS) {
+        const u64 key = keys_sh[j];
+        const u32 dd = (u32)(key >> shift) & 0xFF;
+        const u32 g = bin_global[dd] + (j - bin_local[dd]);
+        if (g < n) dst[g] = key;
+        else atomicOr(err, ERR_CAPACITY);
+    }
 }
 
+int g_sort_variant = 1;  // 0: match-based ranking, 1: ballot-based ranking
+
+// ---------------------------------------------------------------------------
 // padded shared-memory index for blocked reads of 16 consecutive u64
 __device__ __forceinline__ u32 pad16(u32 j) { return j + (j >> 4); }
 
@@ -423,6 +544,15 @@ static bool check_err(SortWorkspace &ws, cudaStream_t s, const char *what)
     return true;
 }
 
+bool sort_check(SortWorkspace &ws, cudaStream_t s)
+{
+    if (!ws.err_dirty) return true;
+    ws.err_dirty = false;
+    if (!check_err(ws, s, "sort_keys")) return false;
+    kclock().flush();
+    return true;
+}
+
 int sort_plan(const u32 *hist_host, u64 n, int *digits)
 {
     int np = 0;
@@ -461,10 +591,16 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     u64 *src = keys, *dst = tmp;
     for (int p = 0; p < np; p++) {
         const int d = digits[p];
-        if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * RADIX * sizeof(u32), s))) return false;
+        const u32 pass_tiles = g_sort_variant == 1 ? ceil_div(n, BAL_TILE) : tiles;
+        if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)pass_tiles * RADIX * sizeof(u32), s))) return false;
         kclock().begin(s, &kstats().onesweep_ms);
-        onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
-                                                       ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);
+        if (g_sort_variant == 1)
+            onesweep_ballot_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d,
+                                                                  ws.small + W_HIST + d * RADIX, ws.lookback,
+                                                                  ws.small + W_CTR + p, ws.small + W_ERR);
+        else
+            onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
+                                                           ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);
         kclock().end(s);
         kstats().onesweep_bytes += 16 * n;
         kstats().onesweep_launches++;
@@ -476,8 +612,8 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         stats->passes = np;
         stats->n = n;
     }
-    if (!check_err(ws, s, "sort_keys")) return false;
-    kclock().flush();
+    // errors of the passes stay in the error word; unique_keys reports them
+    ws.err_dirty = true;
     return true;
 }
 
@@ -491,17 +627,25 @@ bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, 
     }
     if (!ws.reserve(n, s)) return false;
     const u32 tiles = ceil_div(n, UNQ_TILE);
-    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_ERR - W_CTR) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_COUNT, 0, sizeof(u32), s))) return false;
+    if (!ws.err_dirty && !CGB_CUDA(cudaMemsetAsync(ws.small + W_ERR, 0, sizeof(u32), s))) return false;
+    ws.err_dirty = false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * sizeof(u32), s))) return false;
     kclock().begin(s, &kstats().unique_ms);
     unique_kernel<<<tiles, UNQ_THREADS, 0, s>>>(in, (u32)n, out, ws.lookback, ws.small + W_CTR,
                                                 ws.small + W_COUNT, ws.small + W_ERR);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    u32 cnt = 0;
-    if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
-    if (!check_err(ws, s, "unique_keys")) return false;
+    u32 ec[2];  // error word, count
+    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, 2 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     kclock().flush();
+    if (ec[0]) {
+        set_error(std::string("sort/unique: device error ") + err_string(ec[0]));
+        return false;
+    }
+    const u32 cnt = ec[1];
     kstats().unique_bytes += 8 * (n + cnt);
     *n_out = cnt;
     return true;
@@ -522,6 +666,7 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     // splits live after the look-back words
     u32 *splits = ws.lookback + ((u64)tiles + 1);
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
+    ws.err_dirty = false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, ((u64)tiles + 1) * sizeof(u32), s))) return false;
     kclock().begin(s, &kstats().merge_ms);
     merge_partition_kernel<<<ceil_div(tiles + 1, 256), 256, 0, s>>>(a, (u32)na, b, (u32)nb, splits, tiles);
@@ -530,10 +675,15 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     kclock().end(s);
     kstats().launches++;
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    u32 cnt = 0;
-    if (!CGB_CUDA(cudaMemcpyAsync(&cnt, ws.small + W_COUNT, sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
-    if (!check_err(ws, s, "merge_unique")) return false;
+    u32 ec[2];  // error word, count
+    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, 2 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     kclock().flush();
+    if (ec[0]) {
+        set_error(std::string("merge_unique: device error ") + err_string(ec[0]));
+        return false;
+    }
+    const u32 cnt = ec[1];
     kstats().merge_bytes += 8 * (total + cnt);
     *n_out = cnt;
     return true;

@@ -53,6 +53,11 @@ struct HostStage {
 
 }  // namespace cgb
 
+namespace cgb {
+extern int g_solve_variant;
+extern int g_sort_variant;
+}
+
 static Engine &E() { return Engine::get(); }
 
 #define CGB_TRY(x)      \
@@ -105,6 +110,18 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         E().index_kind = (int)value;
+    } else if (k == "solve_variant") {
+        if (value < 0 || value > 1) {
+            set_error("cgb_set_option: solve_variant must be 0 (direct) or 1 (warp queue)");
+            return -1;
+        }
+        g_solve_variant = (int)value;
+    } else if (k == "sort_variant") {
+        if (value < 0 || value > 1) {
+            set_error("cgb_set_option: sort_variant must be 0 (match ranking) or 1 (ballot ranking)");
+            return -1;
+        }
+        g_sort_variant = (int)value;
     } else if (k == "bucket_bits") {
         if (value < 0 || value > 30) {
             set_error("cgb_set_option: bucket_bits must be in 0..30");
@@ -123,6 +140,8 @@ long long cgb_get_option(const char *name)
     const std::string k = name ? name : "";
     if (k == "index") return E().index_kind;
     if (k == "bucket_bits") return E().bucket_bits;
+    if (k == "solve_variant") return g_solve_variant;
+    if (k == "sort_variant") return g_sort_variant;
     return -1;
 }
 
@@ -188,7 +207,7 @@ int cgb_sort(uint64_t *d_keys, uint64_t *d_tmp, uint64_t n, int *result_in_tmp, 
     u64 *sorted = nullptr;
     SortStats st;
     CGB_TRY(sort_keys(d_keys, d_tmp, n, &sorted, E().ws, E().stream, &st));
-    CGB_TRY(E().sync());
+    CGB_TRY(sort_check(E().ws, E().stream));
     if (result_in_tmp) *result_in_tmp = (sorted == d_tmp) ? 1 : 0;
     if (passes) *passes = st.passes;
     return 0;
@@ -329,16 +348,21 @@ struct KeepSink : LayerSink {
     }
 };
 
-void fill_gen_stats(cgb_stats *st, const GenTimes &tm)
+// per-phase device times as the difference of two kernel-clock snapshots
+void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const KernelStats &k1)
 {
     if (!st) return;
     st->boards_generated += tm.boards;
-    st->expand_ms += tm.expand_ms;
-    st->sort_ms += tm.sort_ms;
-    st->unique_ms += tm.unique_ms;
-    st->merge_ms += tm.merge_ms;
+    st->expand_ms += (k1.expand_ms - k0.expand_ms) + (k1.spawn_ms - k0.spawn_ms);
+    st->sort_ms += (k1.onesweep_ms - k0.onesweep_ms) + (k1.hist_ms - k0.hist_ms);
+    st->unique_ms += k1.unique_ms - k0.unique_ms;
+    st->merge_ms += k1.merge_ms - k0.merge_ms;
+    st->solve_kernel_ms += k1.solve_ms - k0.solve_ms;
+    st->index_ms += k1.index_ms - k0.index_ms;
     st->sorted_keys += tm.sorted_keys;
     st->sort_key_passes += tm.sort_passes;
+    st->gpu_launches += k1.launches - k0.launches;
+    st->lookups_bytes += k1.solve_bytes - k0.solve_bytes;
 }
 
 }  // namespace
@@ -351,6 +375,7 @@ extern "C" int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, in
     sink.fn = fn;
     sink.user = user;
     GenTimes tm;
+    const KernelStats k0 = kstats();
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -364,7 +389,7 @@ extern "C" int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, in
     cudaEventDestroy(b);
     if (stats) {
         *stats = cgb_stats{};
-        fill_gen_stats(stats, tm);
+        fill_stats(stats, tm, k0, kstats());
         stats->gen_ms = ms;
         stats->total_ms = ms;
         stats->h2d_bytes = n * 8;
@@ -387,7 +412,7 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     sink.fn = layer_fn;
     sink.user = user;
     GenTimes tm;
-    const u64 launches0 = kstats().launches;
+    const KernelStats k0 = kstats();
     cudaEvent_t ev[3];
     for (auto &x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], s);
@@ -410,7 +435,6 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     };
     Solved t2, t4, cur;
     HostStage stage;
-    double solve_kernel_ms = 0, index_ms = 0;
     u64 solved = 0, d2h = sink.d2h;
     if (ok) ok = dev_alloc((void **)&d_ws, ws.size() * 8 + 8, s);
     if (ok && !ws.empty()) ok = CGB_CUDA(cudaMemcpyAsync(d_ws, ws.data(), ws.size() * 8, cudaMemcpyHostToDevice, s));
@@ -429,7 +453,6 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
             break;
         }
         {
-            Timer t(s, &solve_kernel_ms);
             if (precision == 32)
                 ok = solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, rules, e.rt, e.ctr, s);
             else
@@ -461,7 +484,6 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
         cur.ix.vals = cur.vals;
         cur.ix.n = cur.n;
         {
-            Timer t(s, &index_ms);
             ok = build_index(cur.ix, e.index_kind, vbytes, cur.store, e.bucket_bits, e.ctr, s);
         }
         // the s+4 table is no longer needed: free its values, bucket and keys
@@ -490,15 +512,12 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
     cudaEventElapsedTime(&solve_ms, ev[1], ev[2]);
     for (auto &x : ev) cudaEventDestroy(x);
     if (stats) {
-        fill_gen_stats(stats, tm);
-        stats->gpu_launches = kstats().launches - launches0;
+        fill_stats(stats, tm, k0, kstats());
         stats->layers = sink.layers.size();
         stats->boards_solved = solved;
         stats->gen_ms = gen_ms;
         stats->solve_ms = solve_ms;
         stats->total_ms = gen_ms + solve_ms;
-        stats->solve_kernel_ms = solve_kernel_ms;
-        stats->index_ms = index_ms;
         stats->h2d_bytes = n * 8;
         stats->d2h_bytes = d2h;
     }
