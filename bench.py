@@ -273,19 +273,37 @@ def run_ours(args):
     boards = sum(s["boards_generated"] + s["boards_solved"] for s in stats)
     gpu_launches = kst["launches"]
 
-    # ---- FP32 sweep and its error against FP64
+    # ---- FP32 sweep, its error against FP64, and the plain (bisection) FP64 solve
     fp32 = None
     if not args.no_fp32:
         device.reset_kernel_stats()
         s32 = step(32)
         k32 = device.kernel_stats()
-        fp32 = {"value": (s32["boards_generated"] + s32["boards_solved"]) / (s32["total_ms"] / 1000.0),
-                "solve_boards_per_s": s32["boards_solved"] / (k32["solve_ms"] / 1000.0) if k32["solve_ms"] else None,
-                "fp64_solve_boards_per_s": kst["solve_boards"] / (kst["solve_ms"] / 1000.0) if kst["solve_ms"] else None}
-        if fp32["solve_boards_per_s"] and fp32["fp64_solve_boards_per_s"]:
-            fp32["solve_speedup_vs_fp64"] = fp32["solve_boards_per_s"] / fp32["fp64_solve_boards_per_s"]
+        _, _, s0 = device.tablebase(form.initial, form.start, form.end_gen, form.start, form.winstates, 0)
+        errs = s0["layer_errors"]
+        tot_n = sum(n for n, _, _ in errs.values())
+        old_index = device.get_option("index")
+        device.set_option("index", 0)
+        device.reset_kernel_stats()
+        step(64)
+        kplain = device.kernel_stats()
+        device.set_option("index", old_index)
 
-    # ---- end to end through the C ABI, layers and tables copied to host
+        def rate(k):
+            return k["solve_boards"] / (k["solve_ms"] / 1000.0) if k["solve_ms"] else None
+        fp32 = {"value": (s32["boards_generated"] + s32["boards_solved"]) / (s32["total_ms"] / 1000.0),
+                "solve_boards_per_s": rate(k32), "fp64_solve_boards_per_s": rate(kst),
+                "plain_fp64_solve_boards_per_s": rate(kplain),
+                "max_abs_err": max((mx for _, mx, _ in errs.values()), default=0.0),
+                "mean_abs_err": (sum(n * mean for n, _, mean in errs.values()) / tot_n) if tot_n else 0.0,
+                "layers_checked": len(errs),
+                "tolerance": 1e-6}
+        if fp32["solve_boards_per_s"] and fp32["plain_fp64_solve_boards_per_s"]:
+            fp32["solve_speedup_vs_plain_fp64"] = fp32["solve_boards_per_s"] / fp32["plain_fp64_solve_boards_per_s"]
+        if fp32["solve_boards_per_s"] and fp32["fp64_solve_boards_per_s"]:
+            fp32["solve_speedup_vs_fp64_hash"] = fp32["solve_boards_per_s"] / fp32["fp64_solve_boards_per_s"]
+
+    # ---- end to end through the C ABI: every layer and every table copied to host buffers
     e2e = None
     if not args.no_e2e:
         barrier()
@@ -295,7 +313,8 @@ def run_ours(args):
         e2e_wall = time.perf_counter() - t1
         e2e_boards = sum(s["boards_generated"] + s["boards_solved"] for s in se)
         e2e = {"value": e2e_boards / e2e_wall, "unit": "boards/s",
-               "h2d_bytes_per_step": int(se[0]["h2d_bytes"]), "d2h_bytes_per_step": int(se[0]["d2h_bytes"])}
+               "h2d_bytes_per_step": int(se[0]["h2d_bytes"]), "d2h_bytes_per_step": int(se[0]["d2h_bytes"]),
+               "path": "cgb_sweep_run with layer and table callbacks (pinned double buffers, async D2H)"}
 
     # ---- aggregate over ranks: sum of boards / slowest rank
     if dist is not None:

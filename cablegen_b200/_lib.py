@@ -58,6 +58,17 @@ class KernelStats(C.Structure):
 LAYER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_uint64)
 TABLE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_void_p, C.c_uint64, C.c_int)
 
+ERROR_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_uint64, C.c_double, C.c_double)
+
+
+class Sweep(C.Structure):
+    """cgb_sweep (include/cablegen_b200.h)."""
+    _fields_ = [("initial", C.POINTER(C.c_uint64)), ("n_initial", C.c_uint64), ("start", C.c_int),
+                ("end_gen", C.c_int), ("end_solve", C.c_int), ("winstates", C.POINTER(C.c_uint64)),
+                ("n_winstates", C.c_int), ("precision", C.c_int), ("layer_fn", LAYER_FN), ("table_fn", TABLE_FN),
+                ("error_fn", ERROR_FN), ("user", C.c_void_p)]
+
+
 _lib = None
 
 u64 = C.c_uint64
@@ -83,6 +94,7 @@ def _declare(L):
         "cgb_reset_kernel_stats": (C.c_int, []),
         "cgb_solve_layer": (C.c_int, [vp, u64, vp, C.c_int, vp, vp, u64, vp, vp, u64, pu64, C.c_int]),
         "cgb_generate": (C.c_int, [pu64, u64, C.c_int, C.c_int, LAYER_FN, vp, C.POINTER(Stats)]),
+        "cgb_sweep_run": (C.c_int, [C.POINTER(Sweep), C.POINTER(Stats)]),
         "cgb_tablebase": (C.c_int, [pu64, u64, C.c_int, C.c_int, C.c_int, pu64, C.c_int, C.c_int, LAYER_FN,
                                     TABLE_FN, vp, C.POINTER(Stats)]),
     }

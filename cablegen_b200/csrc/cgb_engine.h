@@ -79,4 +79,32 @@ struct Engine {
     void release_buffers();
 };
 
+// ---- shared by the C ABI files (tablebase.cu, sweep.cu) ---------------------
+// pinned staging for device -> host copies of layers and tables
+struct HostStage {
+    void *p = nullptr;
+    u64 bytes = 0;
+    bool reserve(u64 b)
+    {
+        if (b <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        if (!CGB_CUDA(cudaMallocHost(&p, b))) return false;
+        bytes = b;
+        return true;
+    }
+    ~HostStage()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+std::vector<u64> expand_winstates(const u64 *w, int n);
+SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws);
+void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const KernelStats &k1);
+
 }  // namespace cgb
+
+// initialises the engine and default rules if the caller has not
+extern "C" bool ensure_rules_for_api();

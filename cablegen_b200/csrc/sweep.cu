@@ -1,0 +1,329 @@
+// sweep.cu -- generation + solve with every layer resident in HBM.
+//
+// The reference runs generate() (src/generate.c:551-615), writing every layer
+// to disk, then solve() (src/solve.c:172-224), reading them back top-down with
+// the s+2 and s+4 tables in memory.  Here the layers stay on the device
+// (packed in a LayerStore), the solve walks them top-down, and each solved
+// layer is turned into a lookup index for the two layers below it.  Host
+// copies, when asked for, run on a second stream into double-buffered pinned
+// memory and overlap the following layers' kernels.
+//
+// Precision 0 runs the FP64 and the FP32 chains side by side and reports,
+// per layer, the largest and mean |fp32 - fp64|.
+#include "cgb_engine.h"
+#include <algorithm>
+#include <functional>
+#include <cstring>
+#include <map>
+#include <vector>
+
+using namespace cgb;
+
+namespace {
+
+// device -> pinned host copies on the I/O stream, two slots in flight
+struct AsyncOut {
+    cudaStream_t main = nullptr, io = nullptr;
+    struct Slot {
+        HostStage buf;
+        cudaEvent_t ready = nullptr, done = nullptr;
+        std::function<bool(const char *)> cb;
+        bool busy = false;
+    };
+    Slot slot[2];
+    int next = 0;
+    u64 d2h = 0;
+    bool failed = false;
+
+    bool init(cudaStream_t m, cudaStream_t i)
+    {
+        main = m;
+        io = i;
+        for (auto &s : slot)
+            if (!CGB_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming)) ||
+                !CGB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)))
+                return false;
+        return true;
+    }
+    ~AsyncOut()
+    {
+        for (auto &s : slot) {
+            if (s.ready) cudaEventDestroy(s.ready);
+            if (s.done) cudaEventDestroy(s.done);
+        }
+    }
+    bool finish(Slot &s)
+    {
+        if (!s.busy) return true;
+        s.busy = false;
+        if (!CGB_CUDA(cudaEventSynchronize(s.done))) return false;
+        if (!s.cb((const char *)s.buf.p)) {
+            set_error("host callback failed");
+            return false;
+        }
+        return true;
+    }
+    // copy the segments (device pointer, bytes) into one pinned buffer; cb
+    // gets that buffer once the copy is complete
+    bool enqueue(const std::vector<std::pair<const void *, u64>> &segs, std::function<bool(const char *)> cb)
+    {
+        Slot &s = slot[next];
+        next ^= 1;
+        if (!finish(s)) return false;
+        u64 bytes = 16;
+        for (auto &g : segs) bytes += g.second;
+        if (!s.buf.reserve(bytes)) return false;
+        if (!CGB_CUDA(cudaEventRecord(s.ready, main))) return false;
+        if (!CGB_CUDA(cudaStreamWaitEvent(io, s.ready, 0))) return false;
+        u64 off = 0;
+        for (auto &g : segs) {
+            if (g.second && !CGB_CUDA(cudaMemcpyAsync((char *)s.buf.p + off, g.first, g.second,
+                                                      cudaMemcpyDeviceToHost, io)))
+                return false;
+            off += g.second;
+            d2h += g.second;
+        }
+        if (!CGB_CUDA(cudaEventRecord(s.done, io))) return false;
+        s.cb = std::move(cb);
+        s.busy = true;
+        return true;
+    }
+    // later frees on the main stream must not overtake copies still reading
+    bool fence_main()
+    {
+        for (auto &s : slot)
+            if (s.busy && !CGB_CUDA(cudaStreamWaitEvent(main, s.done, 0))) return false;
+        return true;
+    }
+    bool drain() { return finish(slot[next]) && finish(slot[next ^ 1]); }
+};
+
+struct Layer {
+    int sum;
+    u64 *keys;
+    u64 n;
+};
+
+struct StoreSink : LayerSink {
+    std::vector<Layer> layers;
+    LayerStore store;
+    cgb_layer_fn fn = nullptr;
+    void *user = nullptr;
+    AsyncOut *out = nullptr;
+    bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
+    {
+        // the engine's layer buffer is reused by the next layer step: keep an
+        // exact-size copy in the store (8 B/board)
+        Layer L{sum, store.push(n, s), n};
+        *kept = false;
+        if (!L.keys) return false;
+        if (n && !CGB_CUDA(cudaMemcpyAsync(L.keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
+        layers.push_back(L);
+        if (fn) {
+            cgb_layer_fn f = fn;
+            void *u = user;
+            return out->enqueue({{L.keys, n * 8}}, [f, u, sum, n](const char *h) {
+                return f(u, sum, (const uint64_t *)h, n) == 0;
+            });
+        }
+        return true;
+    }
+};
+
+// one precision's solve state: the current layer and the two above it
+struct Chain {
+    int vbytes = 8;
+    struct Solved {
+        int sum = 0;
+        const u64 *keys = nullptr;
+        void *vals = nullptr;
+        u64 n = 0;
+        IndexStorage store;
+        LayerIndex ix;
+    };
+    Solved t2, t4, cur;
+
+    bool solve(Engine &e, const SolveRules &r, cudaStream_t s)
+    {
+        if (!dev_alloc(&cur.vals, cur.n * vbytes + 8, s)) return false;
+        if (vbytes == 4) return solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
+        return solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
+    }
+    bool index(Engine &e, cudaStream_t s)
+    {
+        cur.ix.keys = cur.keys;
+        cur.ix.vals = cur.vals;
+        cur.ix.n = cur.n;
+        return build_index(cur.ix, e.index_kind, vbytes, cur.store, e.bucket_bits, e.ctr, s);
+    }
+    void rotate(cudaStream_t s)
+    {
+        if (t4.vals) dev_free(t4.vals, s);
+        if (t4.store.p) dev_free(t4.store.p, s);
+        t4 = t2;
+        t2 = cur;
+        cur = Solved{};
+    }
+    void release(cudaStream_t s)
+    {
+        for (Solved *x : {&t2, &t4, &cur}) {
+            if (x->vals) dev_free(x->vals, s);
+            if (x->store.p) dev_free(x->store.p, s);
+            *x = Solved{};
+        }
+    }
+};
+
+// max and sum of |a - b| over a layer (a: fp64, b: fp32)
+__global__ void abs_diff_kernel(const double *__restrict__ a, const float *__restrict__ b, u64 n, u64 *max_bits,
+                                double *sum)
+{
+    double m = 0, t = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const double d = fabs(a[i] - (double)b[i]);
+        m = fmax(m, d);
+        t += d;
+    }
+    for (int o = 16; o; o >>= 1) {
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        // non-negative doubles order like their bit patterns
+        atomicMax((unsigned long long *)max_bits, (unsigned long long)__double_as_longlong(m));
+        atomicAdd(sum, t);
+    }
+}
+
+}  // namespace
+
+extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
+{
+    if (!ensure_rules_for_api()) return -1;
+    Engine &e = Engine::get();
+    cudaStream_t s = e.stream;
+    if (stats) *stats = cgb_stats{};
+    if (w->precision != 0 && w->precision != 32 && w->precision != 64) {
+        set_error("cgb_sweep_run: precision must be 64, 32 or 0");
+        return -1;
+    }
+    AsyncOut out;
+    if (!out.init(s, e.io_stream)) return -1;
+    StoreSink sink;
+    sink.fn = w->layer_fn;
+    sink.user = w->user;
+    sink.out = &out;
+    GenTimes tm;
+    const KernelStats k0 = kstats();
+    cudaEvent_t ev[3];
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], s);
+    bool ok = e.generate(w->initial, w->n_initial, w->start, w->end_gen, sink, &tm);
+    cudaEventRecord(ev[1], s);
+
+    // ---- solve, top-down (src/solve.c:203-219) ----
+    std::map<int, size_t> by_sum;
+    for (size_t i = 0; i < sink.layers.size(); i++) by_sum[sink.layers[i].sum] = i;
+    std::vector<u64> ws = expand_winstates(w->winstates, w->n_winstates);
+    u64 *d_ws = nullptr;
+    std::vector<Chain> chains;
+    if (w->precision == 0) {
+        chains.resize(2);
+        chains[0].vbytes = 8;
+        chains[1].vbytes = 4;
+    } else {
+        chains.resize(1);
+        chains[0].vbytes = w->precision == 32 ? 4 : 8;
+    }
+    u64 *d_err = nullptr;  // [max bits, sum]
+    u64 solved = 0;
+    double max_err = 0;
+    if (ok) ok = dev_alloc((void **)&d_ws, ws.size() * 8 + 8, s);
+    if (ok && !ws.empty()) ok = CGB_CUDA(cudaMemcpyAsync(d_ws, ws.data(), ws.size() * 8, cudaMemcpyHostToDevice, s));
+    if (ok && w->precision == 0) ok = dev_alloc((void **)&d_err, 16, s);
+    const SolveRules rules = make_solve_rules(e.rules, d_ws, (int)ws.size());
+    const int lo = std::max(w->end_solve, 0);
+    for (int sum = w->end_gen; ok && sum >= lo && sum > 0; sum -= 2) {
+        auto it = by_sum.find(sum);
+        const u64 *keys = nullptr;
+        u64 n = 0;
+        if (it != by_sum.end()) {
+            keys = sink.layers[it->second].keys;
+            n = sink.layers[it->second].n;
+        }
+        for (auto &c : chains) {
+            c.cur.sum = sum;
+            c.cur.keys = keys;
+            c.cur.n = n;
+            ok = ok && c.solve(e, rules, s);
+        }
+        if (!ok) break;
+        solved += n;
+        if (w->precision == 0 && n) {
+            ok = CGB_CUDA(cudaMemsetAsync(d_err, 0, 16, s));
+            const int grid = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
+            kstats().launches++;
+            abs_diff_kernel<<<grid, 256, 0, s>>>((const double *)chains[0].cur.vals, (const float *)chains[1].cur.vals,
+                                                 n, d_err, (double *)(d_err + 1));
+            u64 h[2];
+            ok = ok && CGB_CUDA(cudaGetLastError()) &&
+                 CGB_CUDA(cudaMemcpyAsync(h, d_err, 16, cudaMemcpyDeviceToHost, s)) &&
+                 CGB_CUDA(cudaStreamSynchronize(s));
+            if (!ok) break;
+            double mx, sm;
+            memcpy(&mx, &h[0], 8);
+            memcpy(&sm, &h[1], 8);
+            max_err = std::max(max_err, mx);
+            if (w->error_fn && w->error_fn(w->user, sum, n, mx, sm / (double)n) != 0) {
+                set_error("error callback failed");
+                ok = false;
+                break;
+            }
+        }
+        if (w->table_fn) {
+            Chain &c = chains[0];
+            const int prec = c.vbytes == 8 ? 64 : 32;
+            cgb_table_fn f = w->table_fn;
+            void *u = w->user;
+            ok = out.enqueue({{keys, n * 8}, {c.cur.vals, n * (u64)c.vbytes}}, [f, u, sum, n, prec](const char *h) {
+                return f(u, sum, (const uint64_t *)h, h + n * 8, n, prec) == 0;
+            });
+            if (!ok) break;
+        }
+        for (auto &c : chains) ok = ok && c.index(e, s);
+        if (!ok) break;
+        // the s+4 layer is no longer needed by anyone
+        ok = out.fence_main();
+        const int gone = chains[0].t4.sum;
+        for (auto &c : chains) c.rotate(s);
+        auto it4 = by_sum.find(gone);
+        if (gone && it4 != by_sum.end() && sink.layers[it4->second].keys) {
+            sink.store.release(sink.layers[it4->second].keys, s);
+            sink.layers[it4->second].keys = nullptr;
+        }
+    }
+    if (ok) ok = out.drain();
+    out.fence_main();
+    for (auto &c : chains) c.release(s);
+    sink.store.clear(s);
+    dev_free(d_ws, s);
+    dev_free(d_err, s);
+    cudaEventRecord(ev[2], s);
+    cudaEventSynchronize(ev[2]);
+    float gen_ms = 0, solve_ms = 0;
+    cudaEventElapsedTime(&gen_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&solve_ms, ev[1], ev[2]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (stats) {
+        fill_stats(stats, tm, k0, kstats());
+        stats->layers = sink.layers.size();
+        stats->boards_solved = solved;
+        stats->gen_ms = gen_ms;
+        stats->solve_ms = solve_ms;
+        stats->total_ms = gen_ms + solve_ms;
+        stats->h2d_bytes = w->n_initial * 8;
+        stats->d2h_bytes = out.d2h;
+        stats->max_abs_err = max_err;
+    }
+    return ok ? 0 : -1;
+}

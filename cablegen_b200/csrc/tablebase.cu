@@ -31,26 +31,6 @@ SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws)
     return s;
 }
 
-// pinned staging for device -> host copies of layers and tables
-struct HostStage {
-    void *p = nullptr;
-    u64 bytes = 0;
-    bool reserve(u64 b)
-    {
-        if (b <= bytes) return true;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        bytes = 0;
-        if (!CGB_CUDA(cudaMallocHost(&p, b))) return false;
-        bytes = b;
-        return true;
-    }
-    ~HostStage()
-    {
-        if (p) cudaFreeHost(p);
-    }
-};
-
 }  // namespace cgb
 
 namespace cgb {
@@ -164,7 +144,7 @@ int cgb_set_rules(const cgb_rules *r)
     return 0;
 }
 
-static bool ensure_rules()
+bool ensure_rules_for_api()
 {
     if (!ensure_init()) return false;
     if (E().rt.move) return true;
@@ -177,7 +157,7 @@ static bool ensure_rules()
 
 int cgb_expand_moves(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t cap, uint64_t *n_out)
 {
-    CGB_TRY(ensure_rules());
+    CGB_TRY(ensure_rules_for_api());
     if (cap < 4 * n) {
         set_error("cgb_expand_moves: the output needs 4n slots");
         return -1;
@@ -251,7 +231,7 @@ extern "C" int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, 
                                const uint64_t *d_k2, const void *d_v2, uint64_t n2, const uint64_t *d_k4,
                                const void *d_v4, uint64_t n4, const uint64_t *h_winstates, int n_winstates)
 {
-    CGB_TRY(ensure_rules());
+    CGB_TRY(ensure_rules_for_api());
     cudaStream_t s = E().stream;
     std::vector<u64> ws = expand_winstates(h_winstates, n_winstates);
     u64 *d_ws = nullptr;
@@ -309,46 +289,10 @@ struct CopyOutSink : LayerSink {
     }
 };
 
-struct Layer {
-    int sum;
-    u64 *keys;
-    u64 n;
-};
-
-struct KeepSink : LayerSink {
-    std::vector<Layer> layers;
-    LayerStore store;
-    cgb_layer_fn fn = nullptr;
-    void *user = nullptr;
-    HostStage stage;
-    u64 d2h = 0;
-    bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
-    {
-        // the layer sits in a buffer sized for the raw move output (4x the
-        // input); keep an exact-size copy so resident layers cost 8 B/board
-        Layer L;
-        L.sum = sum;
-        L.n = n;
-        L.keys = store.push(n, s);
-        if (!L.keys) return false;
-        if (n && !CGB_CUDA(cudaMemcpyAsync(L.keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
-        layers.push_back(L);
-        *kept = false;
-        if (fn) {
-            if (!stage.reserve(n * 8 + 8)) return false;
-            if (n && !CGB_CUDA(cudaMemcpyAsync(stage.p, d, n * 8, cudaMemcpyDeviceToHost, s))) return false;
-            if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
-            d2h += n * 8;
-            if (fn(user, sum, (const u64 *)stage.p, n) != 0) {
-                set_error("layer callback failed");
-                return false;
-            }
-        }
-        return true;
-    }
-};
-
 // per-phase device times as the difference of two kernel-clock snapshots
+}  // namespace
+
+namespace cgb {
 void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const KernelStats &k1)
 {
     if (!st) return;
@@ -365,12 +309,12 @@ void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const 
     st->lookups_bytes += k1.solve_bytes - k0.solve_bytes;
 }
 
-}  // namespace
+}  // namespace cgb
 
 extern "C" int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, int end, cgb_layer_fn fn, void *user,
                             cgb_stats *stats)
 {
-    CGB_TRY(ensure_rules());
+    CGB_TRY(ensure_rules_for_api());
     CopyOutSink sink;
     sink.fn = fn;
     sink.user = user;
@@ -404,123 +348,17 @@ extern "C" int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, i
                              const uint64_t *h_winstates, int n_winstates, int precision, cgb_layer_fn layer_fn,
                              cgb_table_fn table_fn, void *user, cgb_stats *stats)
 {
-    CGB_TRY(ensure_rules());
-    Engine &e = E();
-    cudaStream_t s = e.stream;
-    if (stats) *stats = cgb_stats{};
-    KeepSink sink;
-    sink.fn = layer_fn;
-    sink.user = user;
-    GenTimes tm;
-    const KernelStats k0 = kstats();
-    cudaEvent_t ev[3];
-    for (auto &x : ev) cudaEventCreate(&x);
-    cudaEventRecord(ev[0], s);
-    bool ok = e.generate(h_initial, n, start, end_gen, sink, &tm);
-    cudaEventRecord(ev[1], s);
-
-    // ---- solve, top-down (src/solve.c:203-219) ----
-    std::map<int, size_t> by_sum;
-    for (size_t i = 0; i < sink.layers.size(); i++) by_sum[sink.layers[i].sum] = i;
-    std::vector<u64> ws = expand_winstates(h_winstates, n_winstates);
-    u64 *d_ws = nullptr;
-    const int vbytes = precision == 32 ? 4 : 8;
-    struct Solved {
-        int sum = 0;
-        const u64 *keys = nullptr;
-        void *vals = nullptr;
-        u64 n = 0;
-        IndexStorage store;
-        LayerIndex ix;
-    };
-    Solved t2, t4, cur;
-    HostStage stage;
-    u64 solved = 0, d2h = sink.d2h;
-    if (ok) ok = dev_alloc((void **)&d_ws, ws.size() * 8 + 8, s);
-    if (ok && !ws.empty()) ok = CGB_CUDA(cudaMemcpyAsync(d_ws, ws.data(), ws.size() * 8, cudaMemcpyHostToDevice, s));
-    const SolveRules rules = make_solve_rules(e.rules, d_ws, (int)ws.size());
-    const int lo = std::max(end_solve, 0);
-    for (int sum = end_gen; ok && sum >= lo && sum > 0; sum -= 2) {
-        auto it = by_sum.find(sum);
-        cur = Solved{};
-        cur.sum = sum;
-        if (it != by_sum.end()) {
-            cur.keys = sink.layers[it->second].keys;
-            cur.n = sink.layers[it->second].n;
-        }
-        if (!dev_alloc(&cur.vals, cur.n * vbytes + 8, s)) {
-            ok = false;
-            break;
-        }
-        {
-            if (precision == 32)
-                ok = solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, rules, e.rt, e.ctr, s);
-            else
-                ok = solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, rules, e.rt, e.ctr, s);
-        }
-        if (!ok) break;
-        solved += cur.n;
-        if (table_fn) {
-            const u64 bytes = cur.n * (8 + vbytes);
-            if (!stage.reserve(bytes + 16)) {
-                ok = false;
-                break;
-            }
-            if (cur.n) {
-                ok = CGB_CUDA(cudaMemcpyAsync(stage.p, cur.keys, cur.n * 8, cudaMemcpyDeviceToHost, s)) &&
-                     CGB_CUDA(cudaMemcpyAsync((char *)stage.p + cur.n * 8, cur.vals, cur.n * vbytes,
-                                              cudaMemcpyDeviceToHost, s));
-            }
-            ok = ok && CGB_CUDA(cudaStreamSynchronize(s));
-            if (!ok) break;
-            d2h += bytes;
-            if (table_fn(user, sum, (const u64 *)stage.p, (const char *)stage.p + cur.n * 8, cur.n, precision)) {
-                set_error("table callback failed");
-                ok = false;
-                break;
-            }
-        }
-        cur.ix.keys = cur.keys;
-        cur.ix.vals = cur.vals;
-        cur.ix.n = cur.n;
-        {
-            ok = build_index(cur.ix, e.index_kind, vbytes, cur.store, e.bucket_bits, e.ctr, s);
-        }
-        // the s+4 table is no longer needed: free its values, bucket and keys
-        if (t4.vals) dev_free(t4.vals, s);
-        if (t4.store.p) dev_free(t4.store.p, s);
-        {
-            auto it4 = by_sum.find(t4.sum);
-            if (t4.sum && it4 != by_sum.end() && sink.layers[it4->second].keys) {
-                sink.store.release(sink.layers[it4->second].keys, s);
-                sink.layers[it4->second].keys = nullptr;
-            }
-        }
-        t4 = t2;
-        t2 = cur;
-    }
-    for (Solved *x : {&t2, &t4}) {
-        if (x->vals) dev_free(x->vals, s);
-        if (x->store.p) dev_free(x->store.p, s);
-    }
-    sink.store.clear(s);
-    dev_free(d_ws, s);
-    cudaEventRecord(ev[2], s);
-    cudaEventSynchronize(ev[2]);
-    float gen_ms = 0, solve_ms = 0;
-    cudaEventElapsedTime(&gen_ms, ev[0], ev[1]);
-    cudaEventElapsedTime(&solve_ms, ev[1], ev[2]);
-    for (auto &x : ev) cudaEventDestroy(x);
-    if (stats) {
-        fill_stats(stats, tm, k0, kstats());
-        stats->layers = sink.layers.size();
-        stats->boards_solved = solved;
-        stats->gen_ms = gen_ms;
-        stats->solve_ms = solve_ms;
-        stats->total_ms = gen_ms + solve_ms;
-        stats->h2d_bytes = n * 8;
-        stats->d2h_bytes = d2h;
-    }
-    CGB_TRY(ok);
-    return 0;
+    cgb_sweep w{};
+    w.initial = h_initial;
+    w.n_initial = n;
+    w.start = start;
+    w.end_gen = end_gen;
+    w.end_solve = end_solve;
+    w.winstates = h_winstates;
+    w.n_winstates = n_winstates;
+    w.precision = precision;
+    w.layer_fn = layer_fn;
+    w.table_fn = table_fn;
+    w.user = user;
+    return cgb_sweep_run(&w, stats);
 }

@@ -165,12 +165,14 @@ def generate(initial: Sequence[int], start: int, end: int, keep: bool = True):
 
 def tablebase(initial: Sequence[int], start: int, end_gen: int, end_solve: int, winstates: Sequence[int],
               precision: int = 64, keep_layers: bool = False, keep_tables: bool = False,
-              layer_fn=None, table_fn=None):
-    """Generation + solve with layers resident in HBM.
+              layer_fn=None, table_fn=None, error_fn=None):
+    """Generation + solve with layers resident in HBM (cgb_sweep_run).
 
+    precision 64 / 32, or 0 to run both and report per-layer FP32 errors
+    (error_fn(sum, n, max_abs, mean_abs); also returned as stats['layer_errors']).
     Returns (layers, tables, stats): layers {sum: keys}, tables {sum: (keys, values)} when kept.
     """
-    layers, tables = {}, {}
+    layers, tables, errors = {}, {}, {}
 
     def on_layer(user, s, ptr, n):
         if keep_layers:
@@ -190,13 +192,29 @@ def tablebase(initial: Sequence[int], start: int, end_gen: int, end_solve: int, 
             table_fn(s, kptr, vptr, n, prec)
         return 0
 
+    def on_error(user, s, n, mx, mean):
+        errors[s] = (n, mx, mean)
+        if error_fn is not None:
+            error_fn(s, n, mx, mean)
+        return 0
+
     want_layers = keep_layers or layer_fn is not None
     want_tables = keep_tables or table_fn is not None
-    lcb = _lib.LAYER_FN(on_layer) if want_layers else _lib.LAYER_FN()
-    tcb = _lib.TABLE_FN(on_table) if want_tables else _lib.TABLE_FN()
+    w = _lib.Sweep()
     init_a = (C.c_uint64 * max(len(initial), 1))(*[int(b) for b in initial])
-    ws = (C.c_uint64 * max(len(winstates), 1))(*[int(w) for w in winstates])
+    ws = (C.c_uint64 * max(len(winstates), 1))(*[int(x) for x in winstates])
+    w.initial = init_a
+    w.n_initial = len(initial)
+    w.start, w.end_gen, w.end_solve = start, end_gen, end_solve
+    w.winstates = ws
+    w.n_winstates = len(winstates)
+    w.precision = precision
+    w.layer_fn = _lib.LAYER_FN(on_layer) if want_layers else _lib.LAYER_FN()
+    w.table_fn = _lib.TABLE_FN(on_table) if want_tables else _lib.TABLE_FN()
+    w.error_fn = _lib.ERROR_FN(on_error) if precision == 0 else _lib.ERROR_FN()
     st = _lib.Stats()
-    check(lib().cgb_tablebase(init_a, len(initial), start, end_gen, end_solve, ws, len(winstates), precision,
-                              lcb, tcb, None, C.byref(st)))
-    return layers, tables, st.as_dict()
+    check(lib().cgb_sweep_run(C.byref(w), C.byref(st)))
+    stats = st.as_dict()
+    if precision == 0:
+        stats["layer_errors"] = errors
+    return layers, tables, stats

@@ -120,6 +120,27 @@ typedef int (*cgb_layer_fn)(void *user, int sum, const uint64_t *h_boards, uint6
 typedef int (*cgb_table_fn)(void *user, int sum, const uint64_t *h_keys, const void *h_values, uint64_t n,
                             int precision);
 
+/* Per-layer FP32-vs-FP64 report of a sweep run with precision 0. */
+typedef int (*cgb_error_fn)(void *user, int sum, uint64_t n, double max_abs, double mean_abs);
+
+/* A generation + solve sweep with every layer resident in HBM. */
+typedef struct {
+    const uint64_t *initial;   /* host boards, all of tile sum `start` */
+    uint64_t n_initial;
+    int start, end_gen, end_solve;
+    const uint64_t *winstates; /* host winstate patterns (expanded to 8 images inside) */
+    int n_winstates;
+    int precision;             /* 64, 32, or 0: both, FP32 compared with FP64 layer by layer */
+    cgb_layer_fn layer_fn;     /* optional: every layer copied to the host */
+    cgb_table_fn table_fn;     /* optional: every table copied to the host (FP64 when precision 0) */
+    cgb_error_fn error_fn;     /* optional, precision 0: per-layer max/mean |fp32 - fp64| */
+    void *user;
+} cgb_sweep;
+/* Copies to the host run on a second stream into double-buffered pinned
+ * memory and overlap the next layers' kernels; the callbacks run on the
+ * calling thread. */
+int cgb_sweep_run(const cgb_sweep *sweep, cgb_stats *stats);
+
 /* Generation sweep from h_initial (all of tile sum `start`) up to `end`
  * (generate(), src/generate.c:551-615); every layer goes to fn. */
 int cgb_generate(const uint64_t *h_initial, uint64_t n, int start, int end, cgb_layer_fn fn, void *user,

@@ -52,6 +52,7 @@ def test_tablebase_fp64_bit_exact(cuda, name, index_kind):
 
 @pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
 def test_tablebase_fp32_error(cuda, index_kind):
+    """FP32 tables with Kahan sums stay within 1e-6 of FP64 (max-abs, every layer)."""
     w = configs.get("plain_2x4_nearwall")
     f = w.formations[0]
     cuda.set_rules(w.settings)
@@ -59,6 +60,33 @@ def test_tablebase_fp32_error(cuda, index_kind):
     _, t32, _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=32, keep_tables=True)
     err = max((np.abs(t64[s][1] - t32[s][1].astype(np.float64)).max() if len(t64[s][1]) else 0.0) for s in t64)
     assert err <= 1e-6, err
+    # the side-by-side mode reports the same per-layer errors and still emits FP64 tables
+    _, tb, st = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=0, keep_tables=True)
+    errs = st["layer_errors"]
+    for s, (n, mx, mean) in errs.items():
+        want = np.abs(t64[s][1] - t32[s][1].astype(np.float64))
+        assert n == len(want) and mx == pytest.approx(want.max(), abs=0) and mean <= mx + 1e-18
+        assert np.array_equal(tb[s][1], t64[s][1])
+    assert st["max_abs_err"] == pytest.approx(err, abs=0)
+
+
+def test_tablebase_async_copies_match(cuda):
+    """Layers and tables copied out asynchronously equal the engine's own (LL, pruned, 40 layers)."""
+    w = configs.get("ll_pruned", end_gen=96)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    lut = O.make_lut(0, 0)
+    ost = O.settings(w.settings)
+    want = O.generate(lut, ost, f.initial, f.start, 96)
+    layers, tables, st = cuda.tablebase(f.initial, f.start, 96, f.start, f.winstates, precision=64,
+                                        keep_layers=True, keep_tables=True)
+    for s in want:
+        assert np.array_equal(layers[s], want[s]), s
+        assert np.array_equal(tables[s][0], want[s]), s
+    vals = O.solve(lut, ost, want, f.winstates, 96, f.start)
+    for s in want:
+        assert np.array_equal(tables[s][1], vals[s]), s
+    assert st["d2h_bytes"] == sum(16 * len(v) for v in want.values()) + sum(8 * len(v) for v in want.values())
 
 
 @pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
