@@ -76,5 +76,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+CLI = os.path.join(OUT_DIR, "cli_b200")
+
+
+def build_cli(reference: str, verbose: bool = False) -> str:
+    """Link the reference's own CLI sources (frontends/cli/main.c, parse.c),
+    unmodified, against this library: the drop-in check of the C API."""
+    src = os.path.join(reference, "frontends", "cli")
+    if not os.path.exists(os.path.join(src, "main.c")):
+        raise FileNotFoundError(src)
+    build()
+    cc = os.environ.get("CC") or shutil.which("gcc") or "cc"
+    cmd = [cc, "-std=c2x", "-O2", "-w", f"-I{ROOT}/include", os.path.join(src, "main.c"), os.path.join(src, "parse.c"),
+           "-o", CLI, f"-L{HERE}", "-lcablegen_b200", "-Wl,-rpath,$ORIGIN/..", "-lm", "-lpthread"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return CLI
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -46,6 +46,29 @@ struct LayerSink {
     virtual bool layer(int sum, u64 *d_boards, u64 n, cudaStream_t s, bool *kept) = 0;
 };
 
+// pinned staging for device -> host copies of layers and tables
+struct HostStage {
+    void *p = nullptr;
+    u64 bytes = 0;
+    // grows with 50 % headroom: pinning memory is slow, so a sequence of
+    // growing layers reallocates only a few times
+    bool reserve(u64 b)
+    {
+        if (b <= bytes) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        const u64 want = b + b / 2;
+        if (!CGB_CUDA(cudaMallocHost(&p, want))) return false;
+        bytes = want;
+        return true;
+    }
+    ~HostStage()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
 // working buffers of the generation sweep, kept between layers and calls
 struct GenBuffers {
     DevBuf<u64> a, b;          // raw move output and its sort scratch
@@ -73,6 +96,7 @@ struct Engine {
     bool sync();
 
     GenBuffers gen;
+    HostStage out_stage[2];     // pinned double buffer of the sweep's host copies
     bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
     bool spawn_layer(GenTimes *tm);
     bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm);
@@ -80,26 +104,6 @@ struct Engine {
 };
 
 // ---- shared by the C ABI files (tablebase.cu, sweep.cu) ---------------------
-// pinned staging for device -> host copies of layers and tables
-struct HostStage {
-    void *p = nullptr;
-    u64 bytes = 0;
-    bool reserve(u64 b)
-    {
-        if (b <= bytes) return true;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        bytes = 0;
-        if (!CGB_CUDA(cudaMallocHost(&p, b))) return false;
-        bytes = b;
-        return true;
-    }
-    ~HostStage()
-    {
-        if (p) cudaFreeHost(p);
-    }
-};
-
 std::vector<u64> expand_winstates(const u64 *w, int n);
 SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws);
 void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const KernelStats &k1);

@@ -25,7 +25,7 @@ namespace {
 struct AsyncOut {
     cudaStream_t main = nullptr, io = nullptr;
     struct Slot {
-        HostStage buf;
+        HostStage *buf = nullptr;
         cudaEvent_t ready = nullptr, done = nullptr;
         std::function<bool(const char *)> cb;
         bool busy = false;
@@ -35,10 +35,12 @@ struct AsyncOut {
     u64 d2h = 0;
     bool failed = false;
 
-    bool init(cudaStream_t m, cudaStream_t i)
+    bool init(cudaStream_t m, cudaStream_t i, HostStage *stages)
     {
         main = m;
         io = i;
+        slot[0].buf = &stages[0];
+        slot[1].buf = &stages[1];
         for (auto &s : slot)
             if (!CGB_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming)) ||
                 !CGB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)))
@@ -57,7 +59,7 @@ struct AsyncOut {
         if (!s.busy) return true;
         s.busy = false;
         if (!CGB_CUDA(cudaEventSynchronize(s.done))) return false;
-        if (!s.cb((const char *)s.buf.p)) {
+        if (!s.cb((const char *)s.buf->p)) {
             set_error("host callback failed");
             return false;
         }
@@ -72,12 +74,12 @@ struct AsyncOut {
         if (!finish(s)) return false;
         u64 bytes = 16;
         for (auto &g : segs) bytes += g.second;
-        if (!s.buf.reserve(bytes)) return false;
+        if (!s.buf->reserve(bytes)) return false;
         if (!CGB_CUDA(cudaEventRecord(s.ready, main))) return false;
         if (!CGB_CUDA(cudaStreamWaitEvent(io, s.ready, 0))) return false;
         u64 off = 0;
         for (auto &g : segs) {
-            if (g.second && !CGB_CUDA(cudaMemcpyAsync((char *)s.buf.p + off, g.first, g.second,
+            if (g.second && !CGB_CUDA(cudaMemcpyAsync((char *)s.buf->p + off, g.first, g.second,
                                                       cudaMemcpyDeviceToHost, io)))
                 return false;
             off += g.second;
@@ -208,7 +210,7 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         return -1;
     }
     AsyncOut out;
-    if (!out.init(s, e.io_stream)) return -1;
+    if (!out.init(s, e.io_stream, e.out_stage)) return -1;
     StoreSink sink;
     sink.fn = w->layer_fn;
     sink.user = w->user;

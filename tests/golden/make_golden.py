@@ -164,6 +164,52 @@ def cmd_run(args):
         shutil.rmtree(work)
 
 
+# ---------------------------------------------------------------- CLI transcripts
+CLI_WORKLOAD = "plain_2x4_nearwall"
+CLI_LOOKUPS = ["0x33301231ffffffff", "0x12000000ffffffff", "0x1123331ffffffff", "0x30100021ffffffff"]
+CLI_SPAWN_LOOKUPS = ["0x33311231ffffffff"]
+
+
+def cli_prepare(work, cores=2):
+    """Config with relative paths, so transcripts do not depend on the directory."""
+    wl = configs.get(CLI_WORKLOAD)
+    form = wl.formations[0]
+    os.makedirs(os.path.join(work, "boards"), exist_ok=True)
+    os.makedirs(os.path.join(work, "tables"), exist_ok=True)
+    np.array(form.initial, dtype="<u8").tofile(os.path.join(work, "initial"))
+    np.array(form.winstates, dtype="<u8").tofile(os.path.join(work, "winstates"))
+    conf = os.path.join(work, "cablegen.conf")
+    write_conf(conf, wl, form, "./boards/", "./tables/", cores)
+    with open(conf) as f:
+        text = f.read()
+    text = text.replace(os.path.join(work, "initial"), "./initial").replace(os.path.join(work, "winstates"), "./winstates")
+    with open(conf, "w") as f:
+        f.write(text)
+    return "cablegen.conf"
+
+
+def cli_commands():
+    cmds = [["lookup", b] for b in CLI_LOOKUPS] + [["lookup_spawn", b] for b in CLI_SPAWN_LOOKUPS]
+    cmds += [["explore", "./tables/16.tables"], ["read", "./boards/14.boards"]]
+    return cmds
+
+
+def cmd_cli(args):
+    work = tempfile.mkdtemp(prefix="golden_cli_")
+    conf = cli_prepare(work)
+    env = dict(os.environ, XDG_CONFIG_HOME=work)
+    for c in ("generate", "solve"):
+        subprocess.run([REF_CLI, f"-C={conf}", c], check=True, cwd=work, env=env, stdout=subprocess.DEVNULL)
+    store = os.path.join(HERE, "cli")
+    os.makedirs(store, exist_ok=True)
+    for i, c in enumerate(cli_commands()):
+        out = subprocess.run([REF_CLI, f"-C={conf}"] + c, cwd=work, env=env, capture_output=True, text=True).stdout
+        with open(os.path.join(store, f"{i:02d}_{c[0]}.txt"), "w") as f:
+            f.write(out)
+    shutil.rmtree(work)
+    print("cli transcripts:", len(cli_commands()))
+
+
 # ---------------------------------------------------------------- unit vectors
 class MinSettings(C.Structure):
     """min_settings_t (api/cablegen.h:47-59)."""
@@ -323,12 +369,13 @@ def main():
     r.add_argument("--keep", default=None, help="keep the reference's files in this directory")
     r.add_argument("--no-solve", action="store_true")
     r.add_argument("--reuse", action="store_true", help="reuse the boards already generated in --keep")
+    sub.add_parser("cli")
     u = sub.add_parser("units")
     u.add_argument("--n", type=int, default=4096)
     a = ap.parse_args()
     if not os.path.exists(REF_CLI):
         sys.exit("build the reference first: make -C oracle all")
-    {"run": cmd_run, "units": cmd_units}[a.cmd](a)
+    {"run": cmd_run, "units": cmd_units, "cli": cmd_cli}[a.cmd](a)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,56 @@
+"""The reference's own CLI (frontends/cli/main.c, parse.c), unmodified, linked against
+libcablegen_b200.so: generate/solve files bit-exact, lookup/explore/read transcripts
+identical to the reference CLI's, and the self-test passing."""
+import os
+import subprocess
+import sys
+
+import pytest
+
+from helpers import GOLDEN, ROOT, digests
+
+sys.path.insert(0, os.path.join(GOLDEN))
+from make_golden import CLI_WORKLOAD, cli_commands, cli_prepare, sha  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(ROOT, "cablegen_b200", "_build", "cli_b200")
+
+
+@pytest.fixture(scope="module")
+def cli_dir(tmp_path_factory):
+    if not os.path.exists(CLI):
+        pytest.skip("cli_b200 is built only where the reference CLI sources exist")
+    work = str(tmp_path_factory.mktemp("cli"))
+    conf = cli_prepare(work)
+    env = dict(os.environ, XDG_CONFIG_HOME=work)
+    for c in ("generate", "solve"):
+        r = subprocess.run([CLI, f"-C={conf}", c], cwd=work, env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+    return work, conf, env
+
+
+def test_cli_files_match_reference(cli_dir):
+    work, _, _ = cli_dir
+    d = digests(CLI_WORKLOAD)["layers"]
+    for s, rec in d.items():
+        assert sha(os.path.join(work, "boards", f"{s}.boards")) == rec["boards_sha256"], s
+        assert sha(os.path.join(work, "tables", f"{s}.tables")) == rec["tables_sha256"], s
+
+
+@pytest.mark.parametrize("i", range(len(cli_commands())))
+def test_cli_transcripts(cli_dir, i):
+    work, conf, env = cli_dir
+    cmd = cli_commands()[i]
+    out = subprocess.run([CLI, f"-C={conf}"] + cmd, cwd=work, env=env, capture_output=True, text=True,
+                         timeout=120).stdout
+    with open(os.path.join(GOLDEN, "cli", f"{i:02d}_{cmd[0]}.txt")) as f:
+        want = f.read()
+    assert out == want
+
+
+def test_cli_self_test(cli_dir):
+    work, conf, env = cli_dir
+    r = subprocess.run([CLI, f"-C={conf}", "test"], cwd=work, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "All tests passed!" in r.stdout
