@@ -277,8 +277,8 @@ bool Engine::spawn_layer(GenTimes *tm)
         if (!reserve(x, total, s)) return false;
     u64 ns = 0;
     if (!expand_spawns(d_moved, n, g.c[0].p, g.c[1].p, total, &ns, ctr, s)) return false;
-    // round 1 sorts c[0] with c[2] as scratch; round 2 sorts c[1] with the
-    // buffer that round 1 left free
+    // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort c[1]
+    // with the buffer the first sort left free
     int in_idx[2] = {0, 1};
     int spare = 2;
     int out_idx[2];
