@@ -35,7 +35,8 @@ class Stats(C.Structure):
                 ("merge_ms", C.c_double), ("solve_kernel_ms", C.c_double), ("index_ms", C.c_double),
                 ("sorted_keys", C.c_uint64), ("sort_key_passes", C.c_uint64), ("lookups_bytes", C.c_uint64),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("max_abs_err", C.c_double),
-                ("gpu_launches", C.c_uint64)]
+                ("gpu_launches", C.c_uint64), ("spilled_chunks", C.c_uint64), ("restored_chunks", C.c_uint64),
+                ("layer_slices", C.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -36,6 +36,7 @@ struct Timer {
 struct GenTimes {
     double expand_ms = 0, sort_ms = 0, unique_ms = 0, merge_ms = 0;
     u64 boards = 0, sorted_keys = 0, sort_passes = 0;
+    u64 chunks = 0;   // slices of layer steps cut at max_sort_keys
 };
 
 // receives each generated layer (device pointer, valid on stream s)
@@ -76,6 +77,7 @@ struct GenBuffers {
     DevBuf<u64> S;             // boards of the next layer to move
     DevBuf<u64> u2, u4, u4_next;
     DevBuf<u64> moved;         // the current layer
+    DevBuf<u64> t;             // merge scratch of sliced layer steps
 };
 
 struct Engine {
@@ -88,6 +90,9 @@ struct Engine {
     cgb_rules rules{};
     int index_kind = INDEX_HASH;  // lookup structure of solved layers
     int bucket_bits = 22;         // INDEX_BUCKET: bucket count = 2^bits
+    u64 spill_reserve = 24ull << 30;  // free device memory kept before spilling resident layers
+    u64 max_sort_keys = 1ull << 28;   // larger layer steps are cut into chunks and merged
+    u64 store_chunk = 4ull << 30;     // device allocation unit of the resident-layer store
 
     static Engine &get();
     bool init(int dev);
@@ -99,6 +104,8 @@ struct Engine {
     HostStage out_stage[2];     // pinned double buffer of the sweep's host copies
     bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
     bool spawn_layer(GenTimes *tm);
+    bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm);
+    bool merge_into(DevBuf<u64> &acc, const u64 *run, u64 n);
     bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm);
     void release_buffers();
 };

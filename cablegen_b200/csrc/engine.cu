@@ -132,52 +132,118 @@ void dev_free(void *p, cudaStream_t s)
     if (p) cudaFreeAsync(p, s);
 }
 
-// ---- resident layer store ---------------------------------------------------
-u64 *LayerStore::push(u64 n, cudaStream_t s)
+// free device memory plus what the stream-ordered pool holds cached but unused
+u64 device_available_bytes(int dev)
 {
-    const u64 need = n ? n : 1;
-    if (chunks_.empty() || chunks_.back().top + need > chunks_.back().cap) {
-        Chunk c;
-        c.cap = std::max<u64>(need, CHUNK_BYTES / 8);
-        c.top = 0;
-        if (!dev_alloc((void **)&c.base, c.cap * 8, s)) return nullptr;
-        chunks_.push_back(c);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    cudaMemPool_t pool;
+    u64 reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
     }
-    Chunk &c = chunks_.back();
-    u64 *p = c.base + c.top;
-    c.blocks.push_back({p, need, true});
-    c.top += need;
-    return p;
+    return (u64)free_b + (reserved > used ? reserved - used : 0);
 }
 
-void LayerStore::release(const u64 *p, cudaStream_t s)
+// ---- resident layer store ---------------------------------------------------
+bool LayerStore::push(u64 n, cudaStream_t s, Handle *h)
 {
-    for (auto &c : chunks_)
-        for (auto &b : c.blocks)
-            if (b.p == p) b.live = false;
-    // pop released blocks from the top, and empty chunks
-    while (!chunks_.empty()) {
-        Chunk &c = chunks_.back();
-        while (!c.blocks.empty() && !c.blocks.back().live) {
-            c.top -= c.blocks.back().n;
-            c.blocks.pop_back();
-        }
-        if (!c.blocks.empty()) break;
+    const u64 need = n ? n : 1;
+    if (chunks_.empty() || !chunks_.back().base || chunks_.back().top + need > chunks_.back().cap) {
+        Chunk c;
+        c.cap = std::max<u64>(need, chunk_bytes / 8);
+        if (!dev_alloc((void **)&c.base, c.cap * 8, s)) return false;
+        chunks_.push_back(std::move(c));
+    }
+    Chunk &c = chunks_.back();
+    h->chunk = (int)chunks_.size() - 1;
+    h->off = c.top;
+    h->n = n;
+    c.blocks.push_back({c.top, need, true});
+    c.top += need;
+    return true;
+}
+
+u64 *LayerStore::ptr(const Handle &h, cudaStream_t s)
+{
+    if (h.chunk < 0) return nullptr;
+    Chunk &c = chunks_[h.chunk];
+    if (!c.base) {  // spilled: bring the chunk back
+        if (!dev_alloc((void **)&c.base, c.cap * 8, s)) return nullptr;
+        if (c.top && !CGB_CUDA(cudaMemcpyAsync(c.base, c.host, c.top * 8, cudaMemcpyHostToDevice, s))) return nullptr;
+        if (!CGB_CUDA(cudaStreamSynchronize(s))) return nullptr;
+        cudaFreeHost(c.host);
+        c.host = nullptr;
+        restores++;
+    }
+    return c.base + h.off;
+}
+
+bool LayerStore::spill_oldest(cudaStream_t s)
+{
+    // never the last chunk: the generation appends to it
+    for (size_t i = 0; i + 1 < chunks_.size(); i++) {
+        Chunk &c = chunks_[i];
+        if (!c.base || c.top == 0) continue;
+        if (!CGB_CUDA(cudaMallocHost(&c.host, c.top * 8))) return false;
+        if (!CGB_CUDA(cudaMemcpyAsync(c.host, c.base, c.top * 8, cudaMemcpyDeviceToHost, s))) return false;
+        if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
         dev_free(c.base, s);
+        c.base = nullptr;
+        spills++;
+        return true;
+    }
+    return false;
+}
+
+void LayerStore::drop_chunk(Chunk &c, cudaStream_t s)
+{
+    if (c.base) dev_free(c.base, s);
+    if (c.host) cudaFreeHost(c.host);
+    c.base = nullptr;
+    c.host = nullptr;
+    c.blocks.clear();
+    c.top = 0;
+}
+
+void LayerStore::release(const Handle &h, cudaStream_t s)
+{
+    if (h.chunk < 0 || h.chunk >= (int)chunks_.size()) return;
+    Chunk &c = chunks_[h.chunk];
+    for (auto &b : c.blocks)
+        if (b.off == h.off) b.live = false;
+    while (!c.blocks.empty() && !c.blocks.back().live) {
+        c.top -= c.blocks.back().n;
+        c.blocks.pop_back();
+    }
+    if (c.blocks.empty()) drop_chunk(c, s);
+    // drop trailing empty chunks so push() starts a fresh one
+    while (!chunks_.empty() && chunks_.back().blocks.empty()) {
+        drop_chunk(chunks_.back(), s);
         chunks_.pop_back();
     }
 }
 
 void LayerStore::clear(cudaStream_t s)
 {
-    for (auto &c : chunks_) dev_free(c.base, s);
+    for (auto &c : chunks_) drop_chunk(c, s);
     chunks_.clear();
 }
 
 u64 LayerStore::bytes_in_use() const
 {
     u64 b = 0;
-    for (auto &c : chunks_) b += c.top * 8;
+    for (auto &c : chunks_)
+        if (c.base) b += c.top * 8;
+    return b;
+}
+
+u64 LayerStore::bytes_spilled() const
+{
+    u64 b = 0;
+    for (auto &c : chunks_)
+        if (c.host) b += c.top * 8;
     return b;
 }
 
@@ -238,33 +304,70 @@ static bool reserve(DevBuf<u64> &b, u64 n, cudaStream_t s)
     return grow(b, n + n / 4 + 1024, s);
 }
 
-// moved = unique(sort(expand_moves(S)))
+// sort + unique of n raw keys in x (y = scratch); returns the buffer holding
+// the unique keys (the other one is left free)
+bool Engine::sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm)
+{
+    cudaStream_t s = stream;
+    u64 *sorted = x.p;
+    SortStats st;
+    if (!sort_keys(x.p, y.p, n, &sorted, ws, s, &st)) return false;
+    if (tm) {
+        tm->sorted_keys += n;
+        tm->sort_passes += (u64)st.passes * n;
+    }
+    DevBuf<u64> &full = (sorted == x.p) ? x : y;
+    DevBuf<u64> &dst = (sorted == x.p) ? y : x;
+    if (!unique_keys(full.p, n, dst.p, nu, ws, s)) return false;
+    *out = &dst;
+    return true;
+}
+
+// acc = acc u run (both sorted unique), through the scratch buffer t
+bool Engine::merge_into(DevBuf<u64> &acc, const u64 *run, u64 n)
+{
+    cudaStream_t s = stream;
+    GenBuffers &g = gen;
+    if (!reserve(g.t, acc.n + n, s)) return false;
+    u64 nm = 0;
+    if (!merge_unique(acc.p, acc.n, run, n, g.t.p, &nm, ws, s)) return false;
+    std::swap(acc, g.t);
+    acc.n = nm;
+    return true;
+}
+
+// moved = unique(sort(expand_moves(S))); an input whose raw moves exceed
+// max_sort_keys is cut into slices whose sorted unique moves are merged
 bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
 {
     cudaStream_t s = stream;
     GenBuffers &g = gen;
-    const u64 cap = 4 * n;
-    if (!reserve(g.a, cap, s) || !reserve(g.b, cap, s)) return false;
-    u64 nr = 0;
-    if (!expand_moves(d_in, n, g.a.p, cap, &nr, rt, prune_params(), ctr, s)) return false;
-    u64 *sorted = g.a.p;
-    SortStats st;
-    if (!sort_keys(g.a.p, g.b.p, nr, &sorted, ws, s, &st)) return false;
-    if (tm) {
-        tm->sorted_keys += nr;
-        tm->sort_passes += (u64)st.passes * nr;
+    const u64 slice = std::max<u64>(1, max_sort_keys / 4);
+    const bool chunked = n > slice;
+    const u64 m0 = chunked ? slice : n;
+    if (!reserve(g.a, 4 * m0, s) || !reserve(g.b, 4 * m0, s)) return false;
+    if (chunked) g.moved.n = 0;
+    for (u64 off = 0; off < n || (n == 0 && off == 0); off += m0) {
+        const u64 m = std::min(m0, n - off);
+        u64 nr = 0;
+        if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s)) return false;
+        u64 nu = 0;
+        DevBuf<u64> *u = nullptr;
+        if (!sort_unique_step(g.a, g.b, nr, &nu, &u, tm)) return false;
+        if (!chunked) {
+            std::swap(*u, g.moved);   // the layer; the old layer buffer becomes scratch
+            g.moved.n = nu;
+            return true;
+        }
+        if (!merge_into(g.moved, u->p, nu)) return false;
+        if (tm) tm->chunks++;
     }
-    DevBuf<u64> &full = (sorted == g.a.p) ? g.a : g.b;
-    DevBuf<u64> &free_ = (sorted == g.a.p) ? g.b : g.a;
-    u64 nm = 0;
-    if (!unique_keys(full.p, nr, free_.p, &nm, ws, s)) return false;
-    std::swap(free_, g.moved);   // the layer; the old layer buffer becomes scratch
-    g.moved.n = nm;
     return true;
 }
 
 // U2 / U4: sorted unique canonical 2-spawns and 4-spawns of the moved layer;
-// U2 lands in g.u2, U4 in g.u4_next
+// U2 lands in g.u2, U4 in g.u4_next.  Spawn streams longer than max_sort_keys
+// are produced slice by slice and merged.
 bool Engine::spawn_layer(GenTimes *tm)
 {
     cudaStream_t s = stream;
@@ -273,34 +376,47 @@ bool Engine::spawn_layer(GenTimes *tm)
     const u64 n = g.moved.n;
     u64 total = 0;
     if (!count_spawns(d_moved, n, &total, ctr, s)) return false;
+    const bool chunked = total > max_sort_keys;
+    const u64 cap = chunked ? max_sort_keys : total;
     for (auto &x : g.c)
-        if (!reserve(x, total, s)) return false;
-    u64 ns = 0;
-    if (!expand_spawns(d_moved, n, g.c[0].p, g.c[1].p, total, &ns, ctr, s)) return false;
-    // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort c[1]
-    // with the buffer the first sort left free
-    int in_idx[2] = {0, 1};
-    int spare = 2;
-    int out_idx[2];
-    for (int k = 0; k < 2; k++) {
-        DevBuf<u64> &in = g.c[in_idx[k]];
-        u64 *sorted = in.p;
-        SortStats st;
-        if (!sort_keys(in.p, g.c[spare].p, ns, &sorted, ws, s, &st)) return false;
-        if (tm) {
-            tm->sorted_keys += ns;
-            tm->sort_passes += (u64)st.passes * ns;
+        if (!reserve(x, cap, s)) return false;
+    if (chunked) g.u2.n = g.u4_next.n = 0;
+    // first guess of a slice that fits; halved while its count does not
+    u64 step = chunked ? std::max<u64>(1, (u64)((double)n * 0.9 * (double)max_sort_keys / (double)total)) : n;
+    for (u64 off = 0; off < n || (n == 0 && off == 0);) {
+        u64 m = std::min(step, n - off);
+        u64 t = total;
+        if (chunked) {
+            for (;;) {
+                if (!count_spawns(d_moved + off, m, &t, ctr, s)) return false;
+                if (t <= max_sort_keys || m == 1) break;
+                m = (m + 1) / 2;
+            }
+            if (t > max_sort_keys) {
+                set_error("spawn_layer: one board spawns more keys than max_sort_keys");
+                return false;
+            }
         }
-        const int full = (sorted == in.p) ? in_idx[k] : spare;
-        const int dst = (sorted == in.p) ? spare : in_idx[k];
-        u64 nu = 0;
-        if (!unique_keys(g.c[full].p, ns, g.c[dst].p, &nu, ws, s)) return false;
-        g.c[dst].n = nu;
-        out_idx[k] = dst;
-        spare = full;
+        u64 ns = 0;
+        if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s)) return false;
+        // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort
+        // c[1] with the buffer the first sort left free
+        DevBuf<u64> *u2 = nullptr, *u4 = nullptr;
+        u64 n2 = 0, n4 = 0;
+        if (!sort_unique_step(g.c[0], g.c[2], ns, &n2, &u2, tm)) return false;
+        DevBuf<u64> &spare = (u2 == &g.c[0]) ? g.c[2] : g.c[0];
+        if (!sort_unique_step(g.c[1], spare, ns, &n4, &u4, tm)) return false;
+        if (!chunked) {
+            std::swap(g.u2, *u2);
+            g.u2.n = n2;
+            std::swap(g.u4_next, *u4);
+            g.u4_next.n = n4;
+            return true;
+        }
+        if (!merge_into(g.u2, u2->p, n2) || !merge_into(g.u4_next, u4->p, n4)) return false;
+        if (tm) tm->chunks++;
+        off += m;
     }
-    std::swap(g.u2, g.c[out_idx[0]]);
-    std::swap(g.u4_next, g.c[out_idx[1]]);
     return true;
 }
 
@@ -343,7 +459,7 @@ bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, Laye
 void Engine::release_buffers()
 {
     GenBuffers &g = gen;
-    for (DevBuf<u64> *b : {&g.a, &g.b, &g.c[0], &g.c[1], &g.c[2], &g.S, &g.u2, &g.u4, &g.u4_next, &g.moved})
+    for (DevBuf<u64> *b : {&g.a, &g.b, &g.c[0], &g.c[1], &g.c[2], &g.S, &g.u2, &g.u4, &g.u4_next, &g.moved, &g.t})
         drop(*b, stream);
 }
 

@@ -16,7 +16,7 @@ struct SortWorkspace {
     u32 *lookback = nullptr;    // decoupled look-back state
     u64 lookback_bytes = 0;
     bool err_dirty = false;     // a sort left its errors in the word for unique to report
-    bool reserve(u64 n, cudaStream_t s);
+    bool reserve(u64 words, cudaStream_t s);
     void release(cudaStream_t s);
 };
 
@@ -141,18 +141,37 @@ void drop(DevBuf<T> &b, cudaStream_t s)
 // Resident layers of a sweep.  Layers are appended during generation and
 // released top-down during the solve (last in, first out), so they are packed
 // into a few large chunks instead of one allocation per layer; nothing is
-// fragmented by the short-lived working buffers of each layer step.
+// fragmented by the short-lived working buffers of each layer step.  When the
+// device runs short, whole chunks of the oldest layers (the lowest tile sums,
+// which the top-down solve needs last) are spilled to pinned host memory and
+// brought back when a layer in them is needed again.
+u64 device_available_bytes(int dev);
+
 class LayerStore {
   public:
-    static constexpr u64 CHUNK_BYTES = 4ull << 30;
-    u64 *push(u64 n, cudaStream_t s);       // room for n boards (nullptr on failure)
-    void release(const u64 *p, cudaStream_t s);  // frees a pushed block (LIFO fast path)
+    u64 chunk_bytes = 4ull << 30;   // device allocation unit of the store
+    struct Handle {
+        int chunk = -1;
+        u64 off = 0, n = 0;
+    };
+    bool push(u64 n, cudaStream_t s, Handle *h);      // room for n boards
+    u64 *ptr(const Handle &h, cudaStream_t s);         // device address (restores a spilled chunk)
+    void release(const Handle &h, cudaStream_t s);     // frees a pushed block
+    bool spill_oldest(cudaStream_t s);                 // false when nothing can be spilled
     void clear(cudaStream_t s);
     u64 bytes_in_use() const;
+    u64 bytes_spilled() const;
+    u64 spills = 0, restores = 0;
   private:
-    struct Block { u64 *p; u64 n; bool live; };
-    struct Chunk { u64 *base; u64 cap; u64 top; std::vector<Block> blocks; };
+    struct Block { u64 off, n; bool live; };
+    struct Chunk {
+        u64 *base = nullptr;   // device memory (null while spilled)
+        void *host = nullptr;  // pinned copy while spilled
+        u64 cap = 0, top = 0;
+        std::vector<Block> blocks;
+    };
     std::vector<Chunk> chunks_;
+    void drop_chunk(Chunk &c, cudaStream_t s);
 };
 
 }  // namespace cgb

@@ -19,6 +19,7 @@
 // sets ERR_LOOKBACK_TIMEOUT in the error word and finishes without waiting.
 #include "common.cuh"
 #include "engine.h"
+#include <cstring>
 
 namespace cgb {
 
@@ -400,48 +401,105 @@ __device__ __forceinline__ u32 merge_path(const u64 *a, u32 na, const u64 *b, u3
     return lo;
 }
 
-__global__ void merge_partition_kernel(const u64 *__restrict__ a, u32 na, const u64 *__restrict__ b, u32 nb,
-                                       u32 *splits, u32 ntiles)
+// merge runs may exceed 2^30 keys (a layer of a large workload): 64-bit
+// positions and a 64-bit look-back word (2 flag bits, 62-bit count)
+constexpr u64 LB64_AGG = 1ull << 62, LB64_PRE = 2ull << 62, LB64_MASK = (1ull << 62) - 1;
+
+__device__ __forceinline__ u64 ld_relaxed64(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(u64 *p, u64 v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ u64 tile_lookback64(u64 *lookback, u32 tile, u64 count, u32 *err)
+{
+    if (tile == 0) {
+        st_relaxed64(lookback, LB64_PRE | count);
+        return 0;
+    }
+    st_relaxed64(lookback + tile, LB64_AGG | count);
+    u64 excl = 0;
+    int j = (int)tile - 1;
+    u32 spins = 0;
+    while (j >= 0) {
+        const u64 v = ld_relaxed64(lookback + j);
+        const u64 flag = v & ~LB64_MASK;
+        if (flag == 0) {
+            if (++spins > SPIN_LIMIT) {
+                atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            __nanosleep(32);
+            continue;
+        }
+        excl += v & LB64_MASK;
+        if (flag == LB64_PRE) break;
+        j--;
+    }
+    st_relaxed64(lookback + tile, LB64_PRE | (excl + count));
+    return excl;
+}
+
+__device__ __forceinline__ u64 merge_path64(const u64 *a, u64 na, const u64 *b, u64 nb, u64 diag)
+{
+    u64 lo = diag > nb ? diag - nb : 0;
+    u64 hi = diag < na ? diag : na;
+    while (lo < hi) {
+        const u64 mid = (lo + hi) >> 1;
+        if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void merge_partition_kernel(const u64 *__restrict__ a, u64 na, const u64 *__restrict__ b, u64 nb,
+                                       u64 *splits, u32 ntiles)
 {
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > ntiles) return;
-    const u32 diag = min((u64)t * MRG_TILE, (u64)na + nb);
-    splits[t] = merge_path(a, na, b, nb, diag);
+    const u64 diag = min((u64)t * MRG_TILE, na + nb);
+    splits[t] = merge_path64(a, na, b, nb, diag);
 }
 
-__global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__restrict__ a, u32 na,
-                                                                   const u64 *__restrict__ b, u32 nb,
-                                                                   const u32 *__restrict__ splits,
-                                                                   u64 *__restrict__ out, u32 *lookback,
-                                                                   u32 *tile_counter, u32 *out_count, u32 *err)
+__global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__restrict__ a, u64 na,
+                                                                   const u64 *__restrict__ b, u64 nb,
+                                                                   const u64 *__restrict__ splits,
+                                                                   u64 *__restrict__ out, u64 *lookback,
+                                                                   u32 *tile_counter, u64 *out_count, u32 *err)
 {
     __shared__ u64 in_sh[MRG_TILE];
     __shared__ u64 out_sh[MRG_TILE + MRG_TILE / 8];
     __shared__ u32 scan_scratch[33];
     __shared__ u64 last_sh[MRG_THREADS];
-    __shared__ u32 tile_sh, prefix_sh;
+    __shared__ u32 tile_sh;
+    __shared__ u64 prefix_sh;
     if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const u32 tile = tile_sh;
-    const u64 total = (u64)na + nb;
-    const u32 d0 = (u32)min((u64)tile * MRG_TILE, total);
-    const u32 d1 = (u32)min((u64)(tile + 1) * MRG_TILE, total);
-    const u32 a0 = splits[tile], a1 = splits[tile + 1];
-    const u32 b0 = d0 - a0, b1 = d1 - a1;
-    const u32 la = a1 - a0, lb = b1 - b0;
+    const u64 total = na + nb;
+    const u64 d0 = min((u64)tile * MRG_TILE, total);
+    const u64 d1 = min((u64)(tile + 1) * MRG_TILE, total);
+    const u64 a0 = splits[tile], a1 = splits[tile + 1];
+    const u64 b0 = d0 - a0, b1 = d1 - a1;
+    const u32 la = (u32)(a1 - a0), lb = (u32)(b1 - b0);
     for (u32 j = threadIdx.x; j < la; j += MRG_THREADS) in_sh[j] = a[a0 + j];
     for (u32 j = threadIdx.x; j < lb; j += MRG_THREADS) in_sh[la + j] = b[b0 + j];
     __syncthreads();
     const u64 *sa = in_sh, *sb = in_sh + la;
     // the merged element just before this tile
-    bool have_before = d0 > 0;
+    const bool have_before = d0 > 0;
     u64 before = 0;
     if (have_before) {
         if (a0 == 0) before = b[b0 - 1];
         else if (b0 == 0) before = a[a0 - 1];
         else before = max(a[a0 - 1], b[b0 - 1]);
     }
-    const u32 len = d1 - d0;
+    const u32 len = (u32)(d1 - d0);
     const u32 t0 = min((u32)(threadIdx.x * MRG_KPT), len);
     const u32 t1 = min(t0 + MRG_KPT, len);
     u32 ia = merge_path(sa, la, sb, lb, t0);
@@ -450,11 +508,10 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++) {
         if (t0 + i < t1) {
-            bool take_a = ib >= lb || (ia < la && sa[ia] <= sb[ib]);
+            const bool take_a = ib >= lb || (ia < la && sa[ia] <= sb[ib]);
             v[i] = take_a ? sa[ia++] : sb[ib++];
         }
     }
-    // predecessor of this thread's first element
     u64 mylast = 0;
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++)
@@ -490,11 +547,11 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
             out_sh[w + (w >> 3)] = v[i];
             w++;
         }
-    if (threadIdx.x == 0) prefix_sh = tile_lookback(lookback, tile, tile_total, err);
+    if (threadIdx.x == 0) prefix_sh = tile_lookback64(lookback, tile, tile_total, err);
     __syncthreads();
-    const u32 prefix = prefix_sh;
+    const u64 prefix = prefix_sh;
     for (u32 j = threadIdx.x; j < tile_total; j += MRG_THREADS) {
-        if ((u64)prefix + j < total) out[prefix + j] = out_sh[j + (j >> 3)];
+        if (prefix + j < total) out[prefix + j] = out_sh[j + (j >> 3)];
         else atomicOr(err, ERR_CAPACITY);
     }
     if (threadIdx.x == 0 && (u64)(tile + 1) * MRG_TILE >= total) *out_count = prefix + tile_total;
@@ -505,10 +562,11 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
 
 static inline u32 ceil_div(u64 a, u64 b) { return (u32)((a + b - 1) / b); }
 
-bool SortWorkspace::reserve(u64 n, cudaStream_t s)
+// look-back words needed: one per bin per tile for a digit pass (the largest
+// user), one per tile for unique, four per tile for a merge
+bool SortWorkspace::reserve(u64 words, cudaStream_t s)
 {
-    const u64 tiles = (n + MRG_TILE - 1) / MRG_TILE + 2;  // the smallest tile size bounds all
-    const u64 need = tiles * RADIX * sizeof(u32);
+    const u64 need = (words + 64) * sizeof(u32);
     if (need <= lookback_bytes && small) return true;
     if (lookback) cudaFreeAsync(lookback, s);
     lookback = nullptr;
@@ -529,8 +587,9 @@ void SortWorkspace::release(cudaStream_t s)
     lookback_bytes = 0;
 }
 
-// small words: [0,2048) histograms, [2048,2064) tile counters, 2064 err, 2065 count
-static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065;
+// small words: [0,2048) histograms, [2048,2064) tile counters, 2064 err, 2065 count,
+// 2066-2067 a 64-bit count (8-byte aligned)
+static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065, W_COUNT64 = 2066;
 
 static bool check_err(SortWorkspace &ws, cudaStream_t s, const char *what)
 {
@@ -574,7 +633,7 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         set_error("sort_keys: more than 2^30 keys in one call");
         return false;
     }
-    if (!ws.reserve(n, s)) return false;
+    if (!ws.reserve(((n + SORT_TILE - 1) / SORT_TILE + 1) * RADIX, s)) return false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (W_COUNT + 1) * sizeof(u32), s))) return false;
     const int hist_blocks = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
     kclock().begin(s, &kstats().hist_ms);
@@ -625,7 +684,7 @@ bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, 
         set_error("unique_keys: more than 2^30 keys in one call");
         return false;
     }
-    if (!ws.reserve(n, s)) return false;
+    if (!ws.reserve((n + UNQ_TILE - 1) / UNQ_TILE + 1, s)) return false;
     const u32 tiles = ceil_div(n, UNQ_TILE);
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_ERR - W_CTR) * sizeof(u32), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_COUNT, 0, sizeof(u32), s))) return false;
@@ -657,33 +716,36 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     *n_out = 0;
     const u64 total = na + nb;
     if (total == 0) return true;
-    if (total > (u64)LB_MASK) {
-        set_error("merge_unique: more than 2^30 keys in one call");
+    const u64 tiles64 = (total + MRG_TILE - 1) / MRG_TILE;
+    if (tiles64 >= (1ull << 31)) {
+        set_error("merge_unique: too many keys");
         return false;
     }
-    if (!ws.reserve(total, s)) return false;
-    const u32 tiles = ceil_div(total, MRG_TILE);
-    // splits live after the look-back words
-    u32 *splits = ws.lookback + ((u64)tiles + 1);
-    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT + 1 - W_CTR) * sizeof(u32), s))) return false;
+    const u32 tiles = (u32)tiles64;
+    if (!ws.reserve(4 * ((u64)tiles + 1), s)) return false;
+    // 64-bit look-back words, then the splits (both fit in the u32 look-back area)
+    u64 *lb = (u64 *)ws.lookback;
+    u64 *splits = lb + ((u64)tiles + 1);
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT64 + 2 - W_CTR) * sizeof(u32), s))) return false;
     ws.err_dirty = false;
-    if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, ((u64)tiles + 1) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(lb, 0, ((u64)tiles + 1) * sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().merge_ms);
-    merge_partition_kernel<<<ceil_div(tiles + 1, 256), 256, 0, s>>>(a, (u32)na, b, (u32)nb, splits, tiles);
-    merge_unique_kernel<<<tiles, MRG_THREADS, 0, s>>>(a, (u32)na, b, (u32)nb, splits, out, ws.lookback,
-                                                      ws.small + W_CTR, ws.small + W_COUNT, ws.small + W_ERR);
+    merge_partition_kernel<<<ceil_div(tiles + 1, 256), 256, 0, s>>>(a, na, b, nb, splits, tiles);
+    merge_unique_kernel<<<tiles, MRG_THREADS, 0, s>>>(a, na, b, nb, splits, out, lb, ws.small + W_CTR,
+                                                      (u64 *)(ws.small + W_COUNT64), ws.small + W_ERR);
     kclock().end(s);
     kstats().launches++;
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    u32 ec[2];  // error word, count
-    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, 2 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    u32 ec[4];  // error word, (count u32 unused), 64-bit count
+    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, 4 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
     if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     kclock().flush();
     if (ec[0]) {
         set_error(std::string("merge_unique: device error ") + err_string(ec[0]));
         return false;
     }
-    const u32 cnt = ec[1];
+    u64 cnt;
+    memcpy(&cnt, &ec[2], 8);
     kstats().merge_bytes += 8 * (total + cnt);
     *n_out = cnt;
     return true;

@@ -102,8 +102,8 @@ struct AsyncOut {
 
 struct Layer {
     int sum;
-    u64 *keys;
-    u64 n;
+    LayerStore::Handle h;
+    bool live;
 };
 
 struct StoreSink : LayerSink {
@@ -112,21 +112,33 @@ struct StoreSink : LayerSink {
     cgb_layer_fn fn = nullptr;
     void *user = nullptr;
     AsyncOut *out = nullptr;
+    u64 reserve_bytes = 0;   // spill older layers when free device memory drops below this
+    int device = 0;
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
         // the engine's layer buffer is reused by the next layer step: keep an
         // exact-size copy in the store (8 B/board)
-        Layer L{sum, store.push(n, s), n};
         *kept = false;
-        if (!L.keys) return false;
-        if (n && !CGB_CUDA(cudaMemcpyAsync(L.keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
+        Layer L{sum, {}, true};
+        if (!store.push(n, s, &L.h)) return false;
+        u64 *keys = store.ptr(L.h, s);
+        if (!keys) return false;
+        if (n && !CGB_CUDA(cudaMemcpyAsync(keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
         layers.push_back(L);
         if (fn) {
             cgb_layer_fn f = fn;
             void *u = user;
-            return out->enqueue({{L.keys, n * 8}}, [f, u, sum, n](const char *h) {
-                return f(u, sum, (const uint64_t *)h, n) == 0;
-            });
+            if (!out->enqueue({{keys, n * 8}}, [f, u, sum, n](const char *h) {
+                    return f(u, sum, (const uint64_t *)h, n) == 0;
+                }))
+                return false;
+        }
+        // keep room for the next layer steps: the working set grows with the
+        // layer, so the reserve scales with it
+        const u64 want = reserve_bytes + 12 * n * 8;
+        while (device_available_bytes(device) < want) {
+            if (!out->fence_main() || !CGB_CUDA(cudaStreamSynchronize(s))) return false;
+            if (!store.spill_oldest(s)) break;
         }
         return true;
     }
@@ -215,6 +227,9 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
     sink.fn = w->layer_fn;
     sink.user = w->user;
     sink.out = &out;
+    sink.reserve_bytes = e.spill_reserve;
+    sink.store.chunk_bytes = e.store_chunk;
+    sink.device = e.device;
     GenTimes tm;
     const KernelStats k0 = kstats();
     cudaEvent_t ev[3];
@@ -250,8 +265,12 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         const u64 *keys = nullptr;
         u64 n = 0;
         if (it != by_sum.end()) {
-            keys = sink.layers[it->second].keys;
-            n = sink.layers[it->second].n;
+            n = sink.layers[it->second].h.n;
+            keys = sink.store.ptr(sink.layers[it->second].h, s);
+            if (!keys) {
+                ok = false;
+                break;
+            }
         }
         for (auto &c : chains) {
             c.cur.sum = sum;
@@ -299,9 +318,9 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         const int gone = chains[0].t4.sum;
         for (auto &c : chains) c.rotate(s);
         auto it4 = by_sum.find(gone);
-        if (gone && it4 != by_sum.end() && sink.layers[it4->second].keys) {
-            sink.store.release(sink.layers[it4->second].keys, s);
-            sink.layers[it4->second].keys = nullptr;
+        if (gone && it4 != by_sum.end() && sink.layers[it4->second].live) {
+            sink.store.release(sink.layers[it4->second].h, s);
+            sink.layers[it4->second].live = false;
         }
     }
     if (ok) ok = out.drain();
@@ -326,6 +345,8 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         stats->h2d_bytes = w->n_initial * 8;
         stats->d2h_bytes = out.d2h;
         stats->max_abs_err = max_err;
+        stats->spilled_chunks = sink.store.spills;
+        stats->restored_chunks = sink.store.restores;
     }
     return ok ? 0 : -1;
 }

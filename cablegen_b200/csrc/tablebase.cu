@@ -102,6 +102,24 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         g_sort_variant = (int)value;
+    } else if (k == "spill_reserve_mb") {
+        if (value < 0) {
+            set_error("cgb_set_option: spill_reserve_mb must be >= 0");
+            return -1;
+        }
+        E().spill_reserve = (u64)value << 20;
+    } else if (k == "store_chunk_mb") {
+        if (value < 1) {
+            set_error("cgb_set_option: store_chunk_mb must be >= 1");
+            return -1;
+        }
+        E().store_chunk = (u64)value << 20;
+    } else if (k == "max_sort_keys") {
+        if (value < (1 << 16) || value > (1 << 30)) {
+            set_error("cgb_set_option: max_sort_keys must be in [2^16, 2^30]");
+            return -1;
+        }
+        E().max_sort_keys = (u64)value;
     } else if (k == "bucket_bits") {
         if (value < 0 || value > 30) {
             set_error("cgb_set_option: bucket_bits must be in 0..30");
@@ -122,6 +140,9 @@ long long cgb_get_option(const char *name)
     if (k == "bucket_bits") return E().bucket_bits;
     if (k == "solve_variant") return g_solve_variant;
     if (k == "sort_variant") return g_sort_variant;
+    if (k == "spill_reserve_mb") return (long long)(E().spill_reserve >> 20);
+    if (k == "max_sort_keys") return (long long)E().max_sort_keys;
+    if (k == "store_chunk_mb") return (long long)(E().store_chunk >> 20);
     return -1;
 }
 
@@ -305,6 +326,7 @@ void fill_stats(cgb_stats *st, const GenTimes &tm, const KernelStats &k0, const 
     st->index_ms += k1.index_ms - k0.index_ms;
     st->sorted_keys += tm.sorted_keys;
     st->sort_key_passes += tm.sort_passes;
+    st->layer_slices += tm.chunks;
     st->gpu_launches += k1.launches - k0.launches;
     st->lookups_bytes += k1.solve_bytes - k0.solve_bytes;
 }

@@ -38,7 +38,12 @@ int cgb_set_rules(const cgb_rules *rules);
 /* Tuning knobs: "index" = lookup structure of solved layers (0 bisection of the
  * sorted layer as in lookup(), src/solve.c:108-164; 1 top-bits buckets then
  * bisection; 2 open-addressing hash, the default), "bucket_bits" (buckets of
- * kind 1).  cgb_get_option returns -1 for an unknown name. */
+ * kind 1), "solve_variant" (0 one thread per board, 1 warp-compacted),
+ * "sort_variant" (0 match ranking, 1 ballot ranking), "spill_reserve_mb"
+ * (free device memory kept before resident layers spill to host memory),
+ * "max_sort_keys" (larger layer steps are cut into chunks and merged),
+ * "store_chunk_mb" (device allocation unit of the resident-layer store).
+ * cgb_get_option returns -1 for an unknown name. */
 int cgb_set_option(const char *name, long long value);
 long long cgb_get_option(const char *name);
 
@@ -97,6 +102,8 @@ typedef struct {
     uint64_t h2d_bytes, d2h_bytes;
     double max_abs_err;                        /* fp32 runs with check: max |fp32 - fp64| */
     uint64_t gpu_launches;                     /* kernels launched by the library */
+    uint64_t spilled_chunks, restored_chunks;  /* resident-layer chunks moved to / from the host */
+    uint64_t layer_slices;                     /* slices of layer steps cut at max_sort_keys */
 } cgb_stats;
 
 /* Device time (ms, CUDA events around every launch) and algorithmic bytes per

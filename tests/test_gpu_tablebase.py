@@ -112,3 +112,48 @@ def test_solve_layer_matches_oracle(cuda, index_kind):
 def _f(cuda, v):
     import torch
     return torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).cuda()
+
+
+def _hashing_sweep(cuda, w, end):
+    f = w.formations[0]
+    got_layers, got_tables = {}, {}
+
+    def on_layer(s, ptr, n):
+        got_layers[s] = sha_layer(np.ctypeslib.as_array(ptr, shape=(n,)) if n else np.zeros(0, np.uint64))
+
+    def on_table(s, kptr, vptr, n, prec):
+        import ctypes as C
+        k = np.ctypeslib.as_array(kptr, shape=(n,)) if n else np.zeros(0, np.uint64)
+        v = (np.ctypeslib.as_array(C.cast(vptr, C.POINTER(C.c_double)), shape=(n,)) if n
+             else np.zeros(0, np.float64))
+        got_tables[s] = sha_table(k, v)
+
+    _, _, st = cuda.tablebase(f.initial, f.start, end, f.start, f.winstates, precision=64,
+                              layer_fn=on_layer, table_fn=on_table)
+    return got_layers, got_tables, st
+
+
+def test_sliced_steps_and_spilled_layers_bit_exact(cuda):
+    """Sliced layer steps (sorted unique runs merged) and layers spilled to host memory and
+    brought back for the solve give the reference's layers and the unsliced run's tables."""
+    w = configs.get("ll_pruned")
+    cuda.set_rules(w.settings)
+    end = 140
+    base_layers, base_tables, _ = _hashing_sweep(cuda, w, end)
+    names = ("max_sort_keys", "store_chunk_mb", "spill_reserve_mb")
+    old = {k: cuda.get_option(k) for k in names}
+    try:
+        cuda.set_option("max_sort_keys", 1 << 18)
+        cuda.set_option("store_chunk_mb", 8)
+        cuda.set_option("spill_reserve_mb", 1 << 30)
+        layers, tables, st = _hashing_sweep(cuda, w, end)
+    finally:
+        for k, v in old.items():
+            cuda.set_option(k, v)
+    want = digests("ll_pruned")["layers"]
+    for s in range(16, end + 1, 2):
+        assert layers[s] == want[str(s)]["boards_sha256"], s
+    assert layers == base_layers
+    assert tables == base_tables
+    assert st["layer_slices"] > 0
+    assert st["spilled_chunks"] > 0 and st["restored_chunks"] > 0
