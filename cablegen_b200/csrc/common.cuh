@@ -18,6 +18,7 @@ enum : u32 {
     ERR_CAPACITY = 1u << 1,           // an output would exceed its buffer
     ERR_UNSORTED = 1u << 2,           // an input that must be sorted was not
     ERR_TOO_LARGE = 1u << 3,          // a size beyond a kernel's 32-bit counters
+    ERR_COPY_TIMEOUT = 1u << 4,       // a bulk copy into shared memory did not complete
 };
 
 // Bounded spin: a wait on another CTA gives up after this many polls.
@@ -141,5 +142,59 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T *scratch, T *total)
     return r;
 }
 #endif
+
+
+// ---- shared-memory barriers and bulk async copies (sm_90+) -----------------
+// One-dimensional global -> shared bulk copies completed on an mbarrier: the
+// copying thread announces the byte count (expect_tx), the copy engine
+// decrements it, waiters poll the phase parity.  No multicast forms.
+__device__ __forceinline__ u32 smem_addr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, u32 count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// make barrier initialisation and earlier generic-proxy shared accesses
+// visible to the async proxy before a bulk copy is issued
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, u32 bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+                 ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// bytes: multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, u32 bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst_smem)), "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, u32 parity)
+{
+    u32 ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of the given parity; false (and ERR_COPY_TIMEOUT
+// in *err) if it did not complete within SPIN_LIMIT polls
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, u32 parity, u32 *err)
+{
+    for (u32 spins = 0; !mbar_try_wait(bar, parity); spins++) {
+        if (spins > SPIN_LIMIT) {
+            atomicOr(err, ERR_COPY_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
 
 }  // namespace cgb

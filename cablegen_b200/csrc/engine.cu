@@ -50,6 +50,7 @@ std::string err_string(u32 err)
     if (err & ERR_CAPACITY) s += "[output capacity exceeded]";
     if (err & ERR_UNSORTED) s += "[input not sorted]";
     if (err & ERR_TOO_LARGE) s += "[size beyond 32-bit counters]";
+    if (err & ERR_COPY_TIMEOUT) s += "[bulk copy wait timed out]";
     return s.empty() ? "[none]" : s;
 }
 

@@ -97,8 +97,8 @@ int cgb_set_option(const char *name, long long value)
         }
         g_solve_variant = (int)value;
     } else if (k == "sort_variant") {
-        if (value < 0 || value > 1) {
-            set_error("cgb_set_option: sort_variant must be 0 (match ranking) or 1 (ballot ranking)");
+        if (value < 0 || value > 2) {
+            set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking) or 2 (pipelined)");
             return -1;
         }
         g_sort_variant = (int)value;

@@ -39,11 +39,19 @@ def test_expand_spawns(cuda):
     assert cuda.count_spawns(cuda.to_device(boards)) == o2.numel()
 
 
-SIZES = [0, 1, 2, 31, 4095, 4096, 4097, 100_000, 1_000_003]
+SIZES = [0, 1, 2, 31, 4095, 4096, 4097, 8193, 100_000, 1_000_003, 5_000_001]
+
+
+@pytest.fixture(params=[0, 1, 2], ids=["match", "ballot", "pipelined"])
+def sort_variant(cuda, request):
+    old = cuda.get_option("sort_variant")
+    cuda.set_option("sort_variant", request.param)
+    yield request.param
+    cuda.set_option("sort_variant", old)
 
 
 @pytest.mark.parametrize("n", SIZES)
-def test_sort_unique_random(cuda, n):
+def test_sort_unique_random(cuda, n, sort_variant):
     rng = np.random.default_rng(n)
     x = rng.integers(0, 1 << 63, size=n, dtype=np.uint64) | (rng.integers(0, 2, size=n, dtype=np.uint64) << np.uint64(63))
     if n > 10:
@@ -54,8 +62,26 @@ def test_sort_unique_random(cuda, n):
     assert np.array_equal(cuda.to_numpy(u), np.unique(x))
 
 
+def test_sort_unaligned_buffers(cuda, sort_variant):
+    """Buffers 8 but not 16 bytes aligned (the pipelined pass falls back to direct loads)."""
+    import ctypes as C
+    import torch
+    from cablegen_b200._lib import check, lib
+    rng = np.random.default_rng(3)
+    n = 700_001
+    x = rng.integers(0, 1 << 63, size=n, dtype=np.uint64)
+    keys = cuda.empty(n + 1)
+    tmp = cuda.empty(n + 1)
+    keys[1:].copy_(cuda.to_device(x))
+    torch.cuda.synchronize()
+    in_tmp, passes = C.c_int(), C.c_int()
+    check(lib().cgb_sort(keys[1:].data_ptr(), tmp[1:].data_ptr(), n, C.byref(in_tmp), C.byref(passes)))
+    out = (tmp if in_tmp.value else keys)[1:]
+    assert np.array_equal(cuda.to_numpy(out), np.sort(x))
+
+
 @pytest.mark.parametrize("kind", ["constant", "sorted", "reversed", "formation", "two_values", "top_bit"])
-def test_sort_skewed(cuda, kind):
+def test_sort_skewed(cuda, kind, sort_variant):
     rng = np.random.default_rng(11)
     n = 300_000
     if kind == "constant":
