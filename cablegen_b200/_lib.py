@@ -70,6 +70,36 @@ class Sweep(C.Structure):
                 ("error_fn", ERROR_FN), ("user", C.c_void_p)]
 
 
+class Formation(C.Structure):
+    """cgb_formation (include/cablegen_b200.h)."""
+    _fields_ = [("initial", C.POINTER(C.c_uint64)), ("n_initial", C.c_uint64), ("end_gen", C.c_int),
+                ("end_solve", C.c_int), ("winstates", C.POINTER(C.c_uint64)), ("n_winstates", C.c_int)]
+
+
+BATCH_LAYER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.c_uint64)
+BATCH_TABLE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.c_void_p,
+                             C.c_uint64, C.c_int)
+
+
+class Batch(C.Structure):
+    """cgb_batch (include/cablegen_b200.h)."""
+    _fields_ = [("formations", C.POINTER(Formation)), ("n_formations", C.c_int), ("precision", C.c_int),
+                ("use_graphs", C.c_int), ("layer_fn", BATCH_LAYER_FN), ("table_fn", BATCH_TABLE_FN),
+                ("user", C.c_void_p)]
+
+
+class BatchStats(C.Structure):
+    """cgb_batch_stats (include/cablegen_b200.h)."""
+    _fields_ = [("groups", C.c_uint64), ("gen_steps", C.c_uint64), ("solve_steps", C.c_uint64),
+                ("boards_generated", C.c_uint64), ("boards_solved", C.c_uint64), ("gen_ms", C.c_double),
+                ("solve_ms", C.c_double), ("total_ms", C.c_double), ("graph_launches", C.c_uint64),
+                ("gpu_launches", C.c_uint64), ("lookups", C.c_uint64), ("h2d_bytes", C.c_uint64),
+                ("d2h_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 u64 = C.c_uint64
@@ -96,6 +126,7 @@ def _declare(L):
         "cgb_solve_layer": (C.c_int, [vp, u64, vp, C.c_int, vp, vp, u64, vp, vp, u64, pu64, C.c_int]),
         "cgb_generate": (C.c_int, [pu64, u64, C.c_int, C.c_int, LAYER_FN, vp, C.POINTER(Stats)]),
         "cgb_sweep_run": (C.c_int, [C.POINTER(Sweep), C.POINTER(Stats)]),
+        "cgb_batch_run": (C.c_int, [C.POINTER(Batch), C.POINTER(BatchStats)]),
         "cgb_tablebase": (C.c_int, [pu64, u64, C.c_int, C.c_int, C.c_int, pu64, C.c_int, C.c_int, LAYER_FN,
                                     TABLE_FN, vp, C.POINTER(Stats)]),
     }

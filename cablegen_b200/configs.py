@@ -226,13 +226,32 @@ def dpdf(seed: int = SEED, end_gen: int = 1200) -> Workload:
         f"DPDF-style formation (cells 2,3,6,7,10,11 fixed), 32 seeded boards, 512 goal, end {end_gen}, prune 58/5/6")
 
 
+def _cell_image(sym: int, cell: int) -> int:
+    """Cell under one of the 8 board symmetries: sym % 4 clockwise quarter turns, then a
+    left-right mirror when sym >= 4."""
+    r, c = divmod(cell, 4)
+    for _ in range(sym % 4):
+        r, c = c, 3 - r
+    if sym >= 4:
+        c = 3 - c
+    return 4 * r + c
+
+
 def batch64(seed: int = SEED, n_formations: int = 64) -> Workload:
+    """Formations whose fixed cells sit at the end of their rows (each row keeps a left-aligned
+    run of free cells), turned by a seeded symmetry: then the moves toward the fixed cells are
+    always legal (fixed cells never move under free_formation off), so every formation grows real
+    layers, while rows of different widths give masks with distinct symmetry orbits."""
     rng = SplitMix64(seed ^ 0xB64)
     forms = []
     for fi in range(n_formations):
         n_free = 6 + rng.below(5)
-        cells = list(range(16))
-        free = sorted(_distinct_cells(rng, cells, n_free))
+        while True:
+            widths = [rng.below(5) for _ in range(4)]
+            if sum(widths) == n_free:
+                break
+        sym = rng.below(8)
+        free = sorted(_cell_image(sym, 4 * r + c) for r in range(4) for c in range(widths[r]))
         fixed = tuple(c for c in range(16) if c not in free)
         goal_exp = 6 + rng.below(3)
         goal_cell = free[rng.below(len(free))]

@@ -168,6 +168,28 @@ __host__ __device__ __forceinline__ int tile_sum(u64 b)
     return s;
 }
 
+// 16-bit mask of the cells holding 0xf (a fixed formation cell): bit i is set
+// when nibble i, counted from the least significant nibble, is 0xf.  With
+// fixed cells that never move, the mask of a canonical board is one of the 8
+// images of its formation's mask, so it tells formations with disjoint mask
+// orbits apart.
+__host__ __device__ __forceinline__ u32 fixed_pattern(u64 b)
+{
+    u64 x = b & (b >> 1) & (b >> 2) & (b >> 3) & 0x1111111111111111ull;
+    x = (x | (x >> 3)) & 0x0303030303030303ull;
+    x = (x | (x >> 6)) & 0x000F000F000F000Full;
+    x = (x | (x >> 12)) & 0x000000FF000000FFull;
+    x = (x | (x >> 24)) & 0xFFFFull;
+    return (u32)x;
+}
+
+// batched sweeps: formation id of a board from its fixed-cell mask (0xff: no
+// formation of the batch) and whether that formation still generates
+struct FormationFilter {
+    const unsigned char *fid = nullptr;     // 65536 entries, by fixed_pattern()
+    const unsigned char *active = nullptr;  // 256 entries
+};
+
 // prune predicate (src/generate.c:98-131).  It depends only on the multiset of
 // tile values, so it may be evaluated on any orientation of the board.
 struct PruneParams {

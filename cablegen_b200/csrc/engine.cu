@@ -351,7 +351,7 @@ bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
     for (u64 off = 0; off < n || (n == 0 && off == 0); off += m0) {
         const u64 m = std::min(m0, n - off);
         u64 nr = 0;
-        if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s)) return false;
+        if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s, filter)) return false;
         u64 nu = 0;
         DevBuf<u64> *u = nullptr;
         if (!sort_unique_step(g.a, g.b, nr, &nu, &u, tm)) return false;

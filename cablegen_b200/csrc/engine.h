@@ -54,8 +54,12 @@ struct Counters {
 };
 
 // move + prune + canonicalise every board; out needs room for 4n boards
+// batched sweeps: stable partition by formation id (fid table of 65536
+// entries, see fixed_pattern); counts[f] = boards of formation f
+bool partition_by_formation(const u64 *in, u64 n, u64 *out, const unsigned char *fid, u32 counts[256],
+                            SortWorkspace &ws, cudaStream_t s);
 bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
-                  const PruneParams &p, Counters &c, cudaStream_t s);
+                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff = FormationFilter{});
 // number of empty cells over all boards (exact size of the spawn streams)
 bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s);
 // canonical 2-spawn and 4-spawn of every empty cell of every board
@@ -68,6 +72,10 @@ struct SolveRules {
     int score = 0;
     const u64 *winstates = nullptr;  // device, expanded x8
     int n_winstates = 0;
+    // batched sweeps: formation f's winstates are winstates[ws_begin[f] ..
+    // ws_begin[f+1]), f = fid[fixed_pattern(board)]
+    const unsigned char *fid = nullptr;
+    const u32 *ws_begin = nullptr;
 };
 
 // Lookup index over one solved layer (replaces the bisection of lookup(),
@@ -98,6 +106,15 @@ struct IndexStorage {
     void *p = nullptr;
     u64 bytes = 0;
 };
+
+// graph-capturable forms (no host round trip): the solve kernel, counting
+// probes into *probes, and the hash index into caller-owned slots
+// (hash_capacity(n) slots of 16 bytes); device errors accumulate in *err
+bool solve_layer_enqueue(const u64 *keys, u64 n, void *out, int vbytes, const LayerIndex &t2, const LayerIndex &t4,
+                         const SolveRules &r, const DeviceRowTable &rt, u64 *probes, cudaStream_t s);
+u64 hash_capacity(u64 n);
+bool solve_prepare();  // one-time kernel attributes (call before a capture)
+bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s);
 
 // builds ix (keys/vals/n already set) of the requested kind; vbytes = 8 or 4
 bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
@@ -160,6 +177,7 @@ class LayerStore {
     bool spill_oldest(cudaStream_t s);                 // false when nothing can be spilled
     void clear(cudaStream_t s);
     u64 bytes_in_use() const;
+    size_t chunk_count() const { return chunks_.size(); }
     u64 bytes_spilled() const;
     u64 spills = 0, restores = 0;
   private:

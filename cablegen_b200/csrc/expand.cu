@@ -93,7 +93,8 @@ __device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned 
 __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
-                                                                      const u32 *g_ok, PruneParams pp, u32 *err)
+                                                                      const u32 *g_ok, PruneParams pp, u32 *err,
+                                                                      FormationFilter ff)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 scan_scratch[33];
@@ -107,7 +108,9 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
         u32 mask = 0;
         if (idx < n) {
             const u64 b = in[idx];
-            if (!(pp.enabled && prune_board(b, pp))) {
+            // boards of a formation that has reached its last layer stop here
+            const bool live = !ff.fid || __ldg(ff.active + __ldg(ff.fid + fixed_pattern(b)));
+            if (live && !(pp.enabled && prune_board(b, pp))) {
                 u64 v[4];
                 views(b, v);
 #pragma unroll
@@ -236,7 +239,7 @@ static bool check(Counters &c, cudaStream_t s, const char *what)
 }
 
 bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
-                  const PruneParams &p, Counters &c, cudaStream_t s)
+                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff)
 {
     *n_out = 0;
     if (n == 0) return true;
@@ -252,7 +255,7 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
     kclock().begin(s, &kstats().expand_ms);
-    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err);
+    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err, ff);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;

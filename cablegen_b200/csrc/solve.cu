@@ -136,7 +136,14 @@ __device__ __forceinline__ bool satisfied(u64 b, const SolveRules &r)
 {
     if (r.nox && !r.score) return has_tile(b, r.nox);
     if (r.score) return false;
-    for (int i = 0; i < r.n_winstates; i++)
+    int lo = 0, hi = r.n_winstates;
+    if (r.fid) {
+        const u32 f = __ldg(r.fid + fixed_pattern(b));
+        if (f == 0xFF) return false;
+        lo = (int)__ldg(r.ws_begin + f);
+        hi = (int)__ldg(r.ws_begin + f + 1);
+    }
+    for (int i = lo; i < hi; i++)
         if (matches(b, __ldg(r.winstates + i))) return true;
     return false;
 }
@@ -442,7 +449,7 @@ bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int buc
     if (ix.n == 0 || kind == INDEX_BISECT) return true;
     if (kind == INDEX_HASH) {
         // load factor <= 0.45: capacity rounded up to a multiple of 64 slots
-        const u64 cap = ((ix.n * 20 / 9) + 63) / 64 * 64;
+        const u64 cap = hash_capacity(ix.n);
         if (!ensure_storage(st, cap * 16, s)) return false;
         if (!CGB_CUDA(cudaMemsetAsync(st.p, 0, cap * 16, s))) return false;
         if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
@@ -512,29 +519,46 @@ static DevTable<V> dev_table(const LayerIndex &ix)
 
 int g_solve_variant = 0;  // 0: direct (one thread per board), 1: warp-compacted queue
 
-template <typename V>
+static bool solve_attrs()
+{
+    static bool attr = false;
+    if (!attr) {
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           SOLVE_SMEM)) ||
+            !CGB_CUDA(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           SOLVE_SMEM)) ||
+            !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_BYTES_S)) ||
+            !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_BYTES_S)))
+            return false;
+        attr = true;
+    }
+    return true;
+}
+
+// the kernel launch alone: no host round trip, so it may be captured in a graph
+template <class V>
+static void enqueue_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
+                          const SolveRules &r, const DeviceRowTable &rt, u64 *probes, cudaStream_t s)
+{
+    if (g_solve_variant == 1)
+        solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, SOLVE_SMEM, s>>>(
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes);
+    else
+        solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes);
+}
+
+template <class V>
 static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
                          const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
 {
     if (n == 0) return true;
-    static bool attr = false;
-    if (!attr) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           SOLVE_SMEM)))
-            return false;
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           TABLE_BYTES_S)))
-            return false;
-        attr = true;
-    }
+    if (!solve_attrs()) return false;
     if (!CGB_CUDA(cudaMemsetAsync(c.d + 2, 0, sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().solve_ms);
-    if (g_solve_variant == 1)
-        solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, SOLVE_SMEM, s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
-    else
-        solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, c.d + 2);
+    enqueue_solve<V>(keys, n, out, t2, t4, r, rt, c.d + 2, s);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u64 probes = 0;
@@ -548,6 +572,43 @@ static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, c
     // keys in, values out, one key sector and one value sector per probe
     k.solve_bytes += (8 + sizeof(V)) * n + 64 * probes;
     return true;
+}
+
+bool solve_layer_enqueue(const u64 *keys, u64 n, void *out, int vbytes, const LayerIndex &t2, const LayerIndex &t4,
+                         const SolveRules &r, const DeviceRowTable &rt, u64 *probes, cudaStream_t s)
+{
+    if (n == 0) return true;
+    if (!solve_attrs()) return false;
+    if (vbytes == 4) enqueue_solve<float>(keys, n, (float *)out, t2, t4, r, rt, probes, s);
+    else enqueue_solve<double>(keys, n, (double *)out, t2, t4, r, rt, probes, s);
+    KernelStats &k = kstats();
+    k.solve_launches++;
+    k.solve_boards += n;
+    return CGB_CUDA(cudaGetLastError());
+}
+
+bool solve_prepare() { return solve_attrs(); }
+
+u64 hash_capacity(u64 n) { return ((n * 20 / 9) + 63) / 64 * 64; }
+
+bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s)
+{
+    ix.kind = INDEX_BISECT;
+    ix.bucket = nullptr;
+    ix.slots = nullptr;
+    ix.cap = 0;
+    if (ix.n == 0) return true;
+    if (!CGB_CUDA(cudaMemsetAsync(slots, 0, cap * 16, s))) return false;
+    if (vbytes == 8)
+        hash_build_kernel<double><<<grid_for(ix.n, 256, 16), 256, 0, s>>>(ix.keys, (const double *)ix.vals, ix.n,
+                                                                         (ulonglong2 *)slots, cap, err);
+    else
+        hash_build_kernel<float><<<grid_for(ix.n, 256, 16), 256, 0, s>>>(ix.keys, (const float *)ix.vals, ix.n,
+                                                                        (ulonglong2 *)slots, cap, err);
+    ix.kind = INDEX_HASH;
+    ix.slots = slots;
+    ix.cap = cap;
+    return CGB_CUDA(cudaGetLastError());
 }
 
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,

@@ -230,8 +230,20 @@ __global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__res
 constexpr int BAL_KPT = 16;
 constexpr int BAL_TILE = SORT_THREADS * BAL_KPT;  // 4096 keys per tile
 
+// the digit of a pass: 8 bits of the key, or (batched sweeps) the formation
+// id, which orders a layer holding several formations by formation
+struct ShiftDigit {
+    int shift;
+    __device__ __forceinline__ u32 operator()(u64 k) const { return (u32)(k >> shift) & 0xFF; }
+};
+struct FormationDigit {
+    const unsigned char *fid;
+    __device__ __forceinline__ u32 operator()(u64 k) const { return __ldg(fid + fixed_pattern(k)); }
+};
+
+template <class Digit>
 __global__ void __launch_bounds__(SORT_THREADS, 5)
-    onesweep_ballot_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
+    onesweep_ballot_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, Digit digit,
                            const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err)
 {
     __shared__ u64 keys_sh[BAL_TILE];
@@ -255,7 +267,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 5)
 #pragma unroll
     for (int i = 0; i < BAL_KPT; i++) {
         const u32 idx = warp_base + i * 32 + lane;
-        const u32 dd = idx < n ? (u32)(src[idx] >> shift) & 0xFF : 0;
+        const u32 dd = idx < n ? digit(src[idx]) : 0;
         if (i % 4 == 0) dg[i / 4] = dd;
         else dg[i / 4] |= dd << (8 * (i % 4));
     }
@@ -320,7 +332,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 5)
     const u32 tile_n = min((u32)BAL_TILE, n - tile_base);
     for (u32 j = threadIdx.x; j < tile_n; j += SORT_THREADS) {
         const u64 key = keys_sh[j];
-        const u32 dd = (u32)(key >> shift) & 0xFF;
+        const u32 dd = digit(key);
         const u32 g = bin_global[dd] + (j - bin_local[dd]);
         if (g < n) dst[g] = key;
         else atomicOr(err, ERR_CAPACITY);
@@ -834,7 +846,7 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
                 src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX, ws.lookback, ws.small + W_CTR + p,
                 ws.small + W_ERR);
         else if (variant == 1)
-            onesweep_ballot_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d,
+            onesweep_ballot_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, ShiftDigit{8 * d},
                                                                   ws.small + W_HIST + d * RADIX, ws.lookback,
                                                                   ws.small + W_CTR + p, ws.small + W_ERR);
         else
@@ -928,6 +940,54 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     memcpy(&cnt, &ec[2], 8);
     kstats().merge_bytes += 8 * (total + cnt);
     *n_out = cnt;
+    return true;
+}
+
+
+// ---------------------------------------------------------------------------
+// batched sweeps: stable partition of a layer by formation id
+__global__ void __launch_bounds__(256) formation_histogram_kernel(const u64 *__restrict__ keys, u64 n,
+                                                                  const unsigned char *__restrict__ fid,
+                                                                  u32 *__restrict__ hist)
+{
+    __shared__ u32 sh[RADIX];
+    sh[threadIdx.x] = 0;
+    __syncthreads();
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        atomicAdd(&sh[__ldg(fid + fixed_pattern(keys[i]))], 1u);
+    __syncthreads();
+    if (sh[threadIdx.x]) atomicAdd(&hist[threadIdx.x], sh[threadIdx.x]);
+}
+
+bool partition_by_formation(const u64 *in, u64 n, u64 *out, const unsigned char *fid, u32 counts[256],
+                            SortWorkspace &ws, cudaStream_t s)
+{
+    memset(counts, 0, 256 * sizeof(u32));
+    if (n == 0) return true;
+    if (n > (u64)LB_MASK) {
+        set_error("partition_by_formation: more than 2^30 keys in one call");
+        return false;
+    }
+    const u32 tiles = ceil_div(n, BAL_TILE);
+    if (!ws.reserve(((u64)tiles + 1) * RADIX, s)) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (W_COUNT + 1) * sizeof(u32), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * RADIX * sizeof(u32), s))) return false;
+    const int hist_blocks = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 4);
+    formation_histogram_kernel<<<hist_blocks, 256, 0, s>>>(in, n, fid, ws.small + W_HIST);
+    onesweep_ballot_kernel<<<tiles, SORT_THREADS, 0, s>>>(in, out, (u32)n, FormationDigit{fid}, ws.small + W_HIST,
+                                                          ws.lookback, ws.small + W_CTR, ws.small + W_ERR);
+    kstats().launches += 2;
+    if (!CGB_CUDA(cudaGetLastError())) return false;
+    u32 e = 0;
+    if (!CGB_CUDA(cudaMemcpyAsync(counts, ws.small + W_HIST, 256 * sizeof(u32), cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaMemcpyAsync(&e, ws.small + W_ERR, sizeof(u32), cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaStreamSynchronize(s)))
+        return false;
+    ws.err_dirty = false;
+    if (e) {
+        set_error("partition_by_formation: device error " + err_string(e));
+        return false;
+    }
     return true;
 }
 

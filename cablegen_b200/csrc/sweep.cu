@@ -10,6 +10,7 @@
 //
 // Precision 0 runs the FP64 and the FP32 chains side by side and reports,
 // per layer, the largest and mean |fp32 - fp64|.
+#include "async_out.h"
 #include "cgb_engine.h"
 #include <algorithm>
 #include <functional>
@@ -20,85 +21,6 @@
 using namespace cgb;
 
 namespace {
-
-// device -> pinned host copies on the I/O stream, two slots in flight
-struct AsyncOut {
-    cudaStream_t main = nullptr, io = nullptr;
-    struct Slot {
-        HostStage *buf = nullptr;
-        cudaEvent_t ready = nullptr, done = nullptr;
-        std::function<bool(const char *)> cb;
-        bool busy = false;
-    };
-    Slot slot[2];
-    int next = 0;
-    u64 d2h = 0;
-    bool failed = false;
-
-    bool init(cudaStream_t m, cudaStream_t i, HostStage *stages)
-    {
-        main = m;
-        io = i;
-        slot[0].buf = &stages[0];
-        slot[1].buf = &stages[1];
-        for (auto &s : slot)
-            if (!CGB_CUDA(cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming)) ||
-                !CGB_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming)))
-                return false;
-        return true;
-    }
-    ~AsyncOut()
-    {
-        for (auto &s : slot) {
-            if (s.ready) cudaEventDestroy(s.ready);
-            if (s.done) cudaEventDestroy(s.done);
-        }
-    }
-    bool finish(Slot &s)
-    {
-        if (!s.busy) return true;
-        s.busy = false;
-        if (!CGB_CUDA(cudaEventSynchronize(s.done))) return false;
-        if (!s.cb((const char *)s.buf->p)) {
-            set_error("host callback failed");
-            return false;
-        }
-        return true;
-    }
-    // copy the segments (device pointer, bytes) into one pinned buffer; cb
-    // gets that buffer once the copy is complete
-    bool enqueue(const std::vector<std::pair<const void *, u64>> &segs, std::function<bool(const char *)> cb)
-    {
-        Slot &s = slot[next];
-        next ^= 1;
-        if (!finish(s)) return false;
-        u64 bytes = 16;
-        for (auto &g : segs) bytes += g.second;
-        if (!s.buf->reserve(bytes)) return false;
-        if (!CGB_CUDA(cudaEventRecord(s.ready, main))) return false;
-        if (!CGB_CUDA(cudaStreamWaitEvent(io, s.ready, 0))) return false;
-        u64 off = 0;
-        for (auto &g : segs) {
-            if (g.second && !CGB_CUDA(cudaMemcpyAsync((char *)s.buf->p + off, g.first, g.second,
-                                                      cudaMemcpyDeviceToHost, io)))
-                return false;
-            off += g.second;
-            d2h += g.second;
-        }
-        if (!CGB_CUDA(cudaEventRecord(s.done, io))) return false;
-        s.cb = std::move(cb);
-        s.busy = true;
-        return true;
-    }
-    // later frees on the main stream must not overtake copies still reading
-    bool fence_main()
-    {
-        for (auto &s : slot)
-            if (s.busy && !CGB_CUDA(cudaStreamWaitEvent(main, s.done, 0))) return false;
-        return true;
-    }
-    bool drain() { return finish(slot[next]) && finish(slot[next ^ 1]); }
-};
 
 struct Layer {
     int sum;
@@ -112,7 +34,8 @@ struct StoreSink : LayerSink {
     cgb_layer_fn fn = nullptr;
     void *user = nullptr;
     AsyncOut *out = nullptr;
-    u64 reserve_bytes = 0;   // spill older layers when free device memory drops below this
+    u64 reserve_bytes = 0;
+    size_t checked_at = 0;  // store chunks at the last free-memory check
     int device = 0;
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
@@ -135,10 +58,14 @@ struct StoreSink : LayerSink {
         }
         // keep room for the next layer steps: the working set grows with the
         // layer, so the reserve scales with it
-        const u64 want = reserve_bytes + 12 * n * 8;
-        while (device_available_bytes(device) < want) {
-            if (!out->fence_main() || !CGB_CUDA(cudaStreamSynchronize(s))) return false;
-            if (!store.spill_oldest(s)) break;
+        // (the device query is not free: ask only when the store took a new chunk)
+        if (store.chunk_count() != checked_at) {
+            const u64 want = reserve_bytes + 12 * n * 8;
+            while (device_available_bytes(device) < want) {
+                if (!out->fence_main() || !CGB_CUDA(cudaStreamSynchronize(s))) return false;
+                if (!store.spill_oldest(s)) break;
+            }
+            checked_at = store.chunk_count();
         }
         return true;
     }

@@ -218,3 +218,60 @@ def tablebase(initial: Sequence[int], start: int, end_gen: int, end_solve: int, 
     if precision == 0:
         stats["layer_errors"] = errors
     return layers, tables, stats
+
+
+def batch(formations, precision: int = 32, use_graphs: bool = True, keep_layers: bool = False,
+          keep_tables: bool = False, layer_fn=None, table_fn=None):
+    """Many formations in one sweep (cgb_batch_run).
+
+    formations: objects with .initial, .end_gen, .end_solve, .winstates (configs.Formation).
+    Returns (layers, tables, stats): layers {(formation, sum): keys}, tables {(formation, sum): (keys, values)}
+    when kept.
+    """
+    layers, tables = {}, {}
+
+    def on_layer(user, f, s, ptr, n):
+        if keep_layers:
+            layers[(f, s)] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+        if layer_fn is not None:
+            layer_fn(f, s, ptr, n)
+        return 0
+
+    def on_table(user, f, s, kptr, vptr, n, prec):
+        if keep_tables:
+            vt = C.c_double if prec == 64 else C.c_float
+            k = np.ctypeslib.as_array(kptr, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+            v = (np.ctypeslib.as_array(C.cast(vptr, C.POINTER(vt)), shape=(n,)).copy() if n
+                 else np.zeros(0, np.float64 if prec == 64 else np.float32))
+            tables[(f, s)] = (k, v)
+        if table_fn is not None:
+            table_fn(f, s, kptr, vptr, n, prec)
+        return 0
+
+    keep = []
+    arr = (_lib.Formation * max(len(formations), 1))()
+    for i, f in enumerate(formations):
+        init = (C.c_uint64 * max(len(f.initial), 1))(*[int(b) for b in f.initial])
+        ws = (C.c_uint64 * max(len(f.winstates), 1))(*[int(x) for x in f.winstates])
+        keep += [init, ws]
+        arr[i].initial = init
+        arr[i].n_initial = len(f.initial)
+        arr[i].end_gen = int(f.end_gen)
+        arr[i].end_solve = int(getattr(f, "end_solve", 0))
+        arr[i].winstates = ws
+        arr[i].n_winstates = len(f.winstates)
+    b = _lib.Batch()
+    b.formations = arr
+    b.n_formations = len(formations)
+    b.precision = precision
+    b.use_graphs = 1 if use_graphs else 0
+    want_layers = keep_layers or layer_fn is not None
+    want_tables = keep_tables or table_fn is not None
+    lf = _lib.BATCH_LAYER_FN(on_layer) if want_layers else _lib.BATCH_LAYER_FN()
+    tf = _lib.BATCH_TABLE_FN(on_table) if want_tables else _lib.BATCH_TABLE_FN()
+    b.layer_fn = lf
+    b.table_fn = tf
+    st = _lib.BatchStats()
+    _sync()
+    check(lib().cgb_batch_run(C.byref(b), C.byref(st)))
+    return layers, tables, st.as_dict()

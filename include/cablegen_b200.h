@@ -163,6 +163,44 @@ int cgb_tablebase(const uint64_t *h_initial, uint64_t n, int start, int end_gen,
                   const uint64_t *h_winstates, int n_winstates, int precision, cgb_layer_fn layer_fn,
                   cgb_table_fn table_fn, void *user, cgb_stats *stats);
 
+/* ---- batched sweeps: many formations in one run --------------------------
+ * No reference counterpart: the reference runs one formation per generate() /
+ * solve() call.  Every formation of a batch advances one layer per step, all
+ * formations' boards in the same kernels (one expansion, one sort, one merge,
+ * one solve launch per step); the solve steps' launch sequences (gathers,
+ * solve, index build) are captured as CUDA graphs.  Boards of different
+ * formations must differ: formations whose fixed-cell masks are images of one
+ * another under the board symmetries run in separate groups.  Requires
+ * free_formation off (fixed cells never move). */
+typedef struct {
+    const uint64_t *initial;   /* host boards, one formation, one tile sum */
+    uint64_t n_initial;
+    int end_gen, end_solve;    /* layers start..end_gen; solved down to max(end_solve, 0) */
+    const uint64_t *winstates; /* host winstate patterns (expanded to 8 images inside) */
+    int n_winstates;
+} cgb_formation;
+/* formation = index into the batch's formation array */
+typedef int (*cgb_batch_layer_fn)(void *user, int formation, int sum, const uint64_t *h_boards, uint64_t n);
+typedef int (*cgb_batch_table_fn)(void *user, int formation, int sum, const uint64_t *h_keys,
+                                  const void *h_values, uint64_t n, int precision);
+typedef struct {
+    const cgb_formation *formations;
+    int n_formations;
+    int precision;             /* 64 or 32 */
+    int use_graphs;            /* 1: capture each solve step as a CUDA graph */
+    cgb_batch_layer_fn layer_fn;
+    cgb_batch_table_fn table_fn;
+    void *user;
+} cgb_batch;
+typedef struct {
+    uint64_t groups, gen_steps, solve_steps;
+    uint64_t boards_generated, boards_solved;
+    double gen_ms, solve_ms, total_ms;
+    uint64_t graph_launches, gpu_launches, lookups;
+    uint64_t h2d_bytes, d2h_bytes;
+} cgb_batch_stats;
+int cgb_batch_run(const cgb_batch *batch, cgb_batch_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif
