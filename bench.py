@@ -13,6 +13,8 @@ Also reported on the same line:
               throughput and its max-abs error against the FP64 tables
   e2e      -- the sweep through the C ABI with every layer and table copied
               to host buffers inside the timed region
+  batch    -- 64 seeded formations in one batched sweep (FP32 solve) against
+              the same formations run one sweep each
   roofline -- the dominant kernel's algorithmic bytes / its CUDA-event time
   cpu_baseline -- the reference's own CPU code on a bounded sample
 
@@ -54,6 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-formation batched sweep block")
     ap.add_argument("--cpu-end", type=int, default=None, help="end tile sum of the CPU sample")
     return ap.parse_args()
 
@@ -316,6 +319,29 @@ def run_ours(args):
                "h2d_bytes_per_step": int(se[0]["h2d_bytes"]), "d2h_bytes_per_step": int(se[0]["d2h_bytes"]),
                "path": "cgb_sweep_run with layer and table callbacks (pinned double buffers, async D2H)"}
 
+    # ---- the 64-formation batch (FP32 solve): one sweep for all formations, and
+    # the same formations run one sweep each
+    batch = None
+    if not args.no_batch:
+        bw = configs.get("batch64")
+        device.set_rules(bw.settings)
+        device.batch(bw.formations, precision=32)  # warm-up
+        _, _, sb = device.batch(bw.formations, precision=32)
+        seq_ms, seq_boards = 0.0, 0
+        for f in bw.formations:
+            _, _, sf = device.tablebase(f.initial, f.start, f.end_gen, f.end_solve, f.winstates, 32)
+            seq_ms += sf["total_ms"]
+            seq_boards += sf["boards_generated"] + sf["boards_solved"]
+        device.set_rules(wl.settings)
+        bb = sb["boards_generated"] + sb["boards_solved"]
+        batch = {"workload": "batch64", "description": bw.description, "formations": len(bw.formations),
+                 "groups": sb["groups"], "solve": "fp32", "boards": bb, "device_ms": sb["total_ms"],
+                 "boards_per_s": bb / (sb["total_ms"] / 1000.0), "graph_launches": sb["graph_launches"],
+                 "gpu_launches": sb["gpu_launches"],
+                 "sequential_boards_per_s": seq_boards / (seq_ms / 1000.0) if seq_ms else None}
+        if batch["sequential_boards_per_s"]:
+            batch["speedup_vs_sequential"] = batch["boards_per_s"] / batch["sequential_boards_per_s"]
+
     # ---- aggregate over ranks: sum of boards / slowest rank
     if dist is not None:
         t = torch.tensor([boards, dev_ms, wall], dtype=torch.float64, device="cuda")
@@ -365,7 +391,7 @@ def run_ours(args):
                            "boards_per_step": boards // max(args.steps, 1),
                            "l2": "inputs larger than L2 (layers resident in HBM, tens of GB)"},
                 "wall_s": wall, "gpu_launches": gpu_launches, "clocks": clock_summary, "roofline": roofline,
-                "fp32": fp32, "e2e": e2e, "cpu_baseline": cpu}
+                "fp32": fp32, "e2e": e2e, "batch": batch, "cpu_baseline": cpu}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
