@@ -127,6 +127,7 @@ def _declare(L):
         "cgb_generate": (C.c_int, [pu64, u64, C.c_int, C.c_int, LAYER_FN, vp, C.POINTER(Stats)]),
         "cgb_sweep_run": (C.c_int, [C.POINTER(Sweep), C.POINTER(Stats)]),
         "cgb_batch_run": (C.c_int, [C.POINTER(Batch), C.POINTER(BatchStats)]),
+        "cgb_batch_plan": (C.c_int, [C.POINTER(Formation), C.c_int, C.POINTER(C.c_int)]),
         "cgb_tablebase": (C.c_int, [pu64, u64, C.c_int, C.c_int, C.c_int, pu64, C.c_int, C.c_int, LAYER_FN,
                                     TABLE_FN, vp, C.POINTER(Stats)]),
     }

@@ -153,10 +153,9 @@ struct BatchSink : LayerSink {
         // (the device query is not free: ask only when the store took a new chunk)
         if (store.chunk_count() != checked_at) {
             const u64 want = reserve_bytes + 12 * n * 8;
-            while (device_available_bytes(e->device) < want) {
-                if (!out->fence_main() || !CGB_CUDA(cudaStreamSynchronize(s))) return false;
-                if (!store.spill_oldest(s)) break;
-            }
+            const u64 avail = device_available_bytes(e->device);
+            // false when nothing is left to spill: carry on, an allocation may still fit
+            if (avail < want) store.spill(want - avail, s, out->io);
             checked_at = store.chunk_count();
         }
         return true;
@@ -410,7 +409,68 @@ bool run_group(Engine &e, const cgb_batch *b, std::vector<Plan> &plans, cgb_batc
     return ok;
 }
 
+// plans of every formation, in groups whose fixed-cell mask orbits are
+// pairwise disjoint (greedy, first group that fits, at most 255 per group)
+bool make_groups(const cgb_formation *fs, int n, std::vector<std::vector<Plan>> &groups, std::vector<int> *group_of)
+{
+    std::vector<Plan> all(n);
+    for (int i = 0; i < n; i++) {
+        const cgb_formation &f = fs[i];
+        Plan &p = all[i];
+        p.index = i;
+        if (f.n_initial == 0 || !f.initial) {
+            set_error("cgb_batch: formation " + std::to_string(i) + " has no initial boards");
+            return false;
+        }
+        p.initial.assign(f.initial, f.initial + f.n_initial);
+        p.start = tile_sum_host(p.initial[0]);
+        p.mask = fixed_pattern(p.initial[0]);
+        for (u64 x : p.initial)
+            if (tile_sum_host(x) != p.start || fixed_pattern(x) != p.mask) {
+                set_error("cgb_batch: formation " + std::to_string(i) +
+                          ": initial boards must share one tile sum and one set of fixed cells");
+                return false;
+            }
+        std::sort(p.initial.begin(), p.initial.end());
+        p.initial.erase(std::unique(p.initial.begin(), p.initial.end()), p.initial.end());
+        p.end_gen = f.end_gen;
+        p.lo_solve = std::max(f.end_solve, 0);
+        p.steps = f.end_gen >= p.start ? (f.end_gen - p.start) / 2 + 1 : 0;
+        p.winstates = expand_winstates(f.winstates, f.n_winstates);
+    }
+    std::vector<std::vector<char>> taken;  // per group: masks used
+    if (group_of) group_of->assign(n, -1);
+    for (auto &p : all) {
+        u32 orbit[8];
+        mask_orbit(p.mask, orbit);
+        size_t g = 0;
+        for (; g < groups.size(); g++) {
+            bool clash = groups[g].size() >= 255;
+            for (u32 m : orbit) clash |= taken[g][m] != 0;
+            if (!clash) break;
+        }
+        if (g == groups.size()) {
+            groups.emplace_back();
+            taken.emplace_back(65536, 0);
+        }
+        for (u32 m : orbit) taken[g][m] = 1;
+        if (group_of) (*group_of)[p.index] = (int)g;
+        groups[g].push_back(std::move(p));
+    }
+    return true;
+}
+
 }  // namespace
+
+extern "C" int cgb_batch_plan(const cgb_formation *formations, int n_formations, int *group_of)
+{
+    std::vector<std::vector<Plan>> groups;
+    std::vector<int> g;
+    if (n_formations < 0 || !make_groups(formations, n_formations, groups, &g)) return -1;
+    if (group_of)
+        for (int i = 0; i < n_formations; i++) group_of[i] = g[i];
+    return (int)groups.size();
+}
 
 extern "C" int cgb_batch_run(const cgb_batch *b, cgb_batch_stats *stats)
 {
@@ -429,50 +489,8 @@ extern "C" int cgb_batch_run(const cgb_batch *b, cgb_batch_stats *stats)
         if (stats) *stats = st;
         return 0;
     }
-    // plans, then groups of formations with pairwise disjoint mask orbits
-    std::vector<Plan> all(b->n_formations);
-    for (int i = 0; i < b->n_formations; i++) {
-        const cgb_formation &f = b->formations[i];
-        Plan &p = all[i];
-        p.index = i;
-        if (f.n_initial == 0) {
-            set_error("cgb_batch_run: formation " + std::to_string(i) + " has no initial boards");
-            return -1;
-        }
-        p.initial.assign(f.initial, f.initial + f.n_initial);
-        p.start = tile_sum_host(p.initial[0]);
-        p.mask = fixed_pattern(p.initial[0]);
-        for (u64 x : p.initial)
-            if (tile_sum_host(x) != p.start || fixed_pattern(x) != p.mask) {
-                set_error("cgb_batch_run: formation " + std::to_string(i) +
-                          ": initial boards must share one tile sum and one set of fixed cells");
-                return -1;
-            }
-        std::sort(p.initial.begin(), p.initial.end());
-        p.initial.erase(std::unique(p.initial.begin(), p.initial.end()), p.initial.end());
-        p.end_gen = f.end_gen;
-        p.lo_solve = std::max(f.end_solve, 0);
-        p.steps = f.end_gen >= p.start ? (f.end_gen - p.start) / 2 + 1 : 0;
-        p.winstates = expand_winstates(f.winstates, f.n_winstates);
-    }
     std::vector<std::vector<Plan>> groups;
-    std::vector<std::vector<char>> taken;  // per group: mask used
-    for (auto &p : all) {
-        u32 orbit[8];
-        mask_orbit(p.mask, orbit);
-        size_t g = 0;
-        for (; g < groups.size(); g++) {
-            bool clash = groups[g].size() >= 255;
-            for (u32 m : orbit) clash |= taken[g][m] != 0;
-            if (!clash) break;
-        }
-        if (g == groups.size()) {
-            groups.emplace_back();
-            taken.emplace_back(65536, 0);
-        }
-        for (u32 m : orbit) taken[g][m] = 1;
-        groups[g].push_back(p);
-    }
+    if (!make_groups(b->formations, b->n_formations, groups, nullptr)) return -1;
     AsyncOut out;
     if (!out.init(e.stream, e.io_stream, e.out_stage)) return -1;
     const KernelStats k0 = kstats();

@@ -172,6 +172,7 @@ u64 *LayerStore::ptr(const Handle &h, cudaStream_t s)
     Chunk &c = chunks_[h.chunk];
     if (!c.base) {  // spilled: bring the chunk back
         if (!dev_alloc((void **)&c.base, c.cap * 8, s)) return nullptr;
+        if (!CGB_CUDA(cudaStreamWaitEvent(s, c.copied, 0))) return nullptr;
         if (c.top && !CGB_CUDA(cudaMemcpyAsync(c.base, c.host, c.top * 8, cudaMemcpyHostToDevice, s))) return nullptr;
         if (!CGB_CUDA(cudaStreamSynchronize(s))) return nullptr;
         cudaFreeHost(c.host);
@@ -181,26 +182,38 @@ u64 *LayerStore::ptr(const Handle &h, cudaStream_t s)
     return c.base + h.off;
 }
 
-bool LayerStore::spill_oldest(cudaStream_t s)
+bool LayerStore::spill(u64 bytes, cudaStream_t s, cudaStream_t io)
 {
+    u64 done = 0;
     // never the last chunk: the generation appends to it
-    for (size_t i = 0; i + 1 < chunks_.size(); i++) {
+    for (size_t i = 0; i + 1 < chunks_.size() && done < bytes; i++) {
         Chunk &c = chunks_[i];
         if (!c.base || c.top == 0) continue;
         if (!CGB_CUDA(cudaMallocHost(&c.host, c.top * 8))) return false;
-        if (!CGB_CUDA(cudaMemcpyAsync(c.host, c.base, c.top * 8, cudaMemcpyDeviceToHost, s))) return false;
-        if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
-        dev_free(c.base, s);
+        if (!c.copied && !CGB_CUDA(cudaEventCreateWithFlags(&c.copied, cudaEventDisableTiming))) return false;
+        cudaEvent_t written;  // the main stream's writes into the chunk
+        if (!CGB_CUDA(cudaEventCreateWithFlags(&written, cudaEventDisableTiming))) return false;
+        const bool ok = CGB_CUDA(cudaEventRecord(written, s)) && CGB_CUDA(cudaStreamWaitEvent(io, written, 0)) &&
+                        CGB_CUDA(cudaMemcpyAsync(c.host, c.base, c.top * 8, cudaMemcpyDeviceToHost, io)) &&
+                        CGB_CUDA(cudaEventRecord(c.copied, io));
+        cudaEventDestroy(written);
+        if (!ok) return false;
+        dev_free(c.base, io);   // back to the pool once the copy has read it
         c.base = nullptr;
+        done += c.cap * 8;
         spills++;
-        return true;
     }
-    return false;
+    return done > 0;
 }
 
 void LayerStore::drop_chunk(Chunk &c, cudaStream_t s)
 {
     if (c.base) dev_free(c.base, s);
+    if (c.copied) {
+        cudaEventSynchronize(c.copied);  // a spill copy may still be reading into c.host
+        cudaEventDestroy(c.copied);
+        c.copied = nullptr;
+    }
     if (c.host) cudaFreeHost(c.host);
     c.base = nullptr;
     c.host = nullptr;

@@ -161,7 +161,9 @@ void drop(DevBuf<T> &b, cudaStream_t s)
 // fragmented by the short-lived working buffers of each layer step.  When the
 // device runs short, whole chunks of the oldest layers (the lowest tile sums,
 // which the top-down solve needs last) are spilled to pinned host memory and
-// brought back when a layer in them is needed again.
+// brought back when a layer in them is needed again.  A spill copies on the
+// I/O stream and frees the device chunk there, stream-ordered after the copy,
+// so the layer loop on the main stream never waits for it.
 u64 device_available_bytes(int dev);
 
 class LayerStore {
@@ -174,7 +176,9 @@ class LayerStore {
     bool push(u64 n, cudaStream_t s, Handle *h);      // room for n boards
     u64 *ptr(const Handle &h, cudaStream_t s);         // device address (restores a spilled chunk)
     void release(const Handle &h, cudaStream_t s);     // frees a pushed block
-    bool spill_oldest(cudaStream_t s);                 // false when nothing can be spilled
+    // spills oldest chunks (never the last) until `bytes` are on their way to
+    // the host; false when nothing could be spilled
+    bool spill(u64 bytes, cudaStream_t s, cudaStream_t io);
     void clear(cudaStream_t s);
     u64 bytes_in_use() const;
     size_t chunk_count() const { return chunks_.size(); }
@@ -185,6 +189,7 @@ class LayerStore {
     struct Chunk {
         u64 *base = nullptr;   // device memory (null while spilled)
         void *host = nullptr;  // pinned copy while spilled
+        cudaEvent_t copied = nullptr;  // the device-to-host copy of the spill is complete
         u64 cap = 0, top = 0;
         std::vector<Block> blocks;
     };

@@ -448,7 +448,7 @@ bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int buc
     ix.cap = 0;
     if (ix.n == 0 || kind == INDEX_BISECT) return true;
     if (kind == INDEX_HASH) {
-        // load factor <= 0.45: capacity rounded up to a multiple of 64 slots
+        // load factor <= g_hash_load_pct: capacity rounded up to a multiple of 64 slots
         const u64 cap = hash_capacity(ix.n);
         if (!ensure_storage(st, cap * 16, s)) return false;
         if (!CGB_CUDA(cudaMemsetAsync(st.p, 0, cap * 16, s))) return false;
@@ -589,7 +589,9 @@ bool solve_layer_enqueue(const u64 *keys, u64 n, void *out, int vbytes, const La
 
 bool solve_prepare() { return solve_attrs(); }
 
-u64 hash_capacity(u64 n) { return ((n * 20 / 9) + 63) / 64 * 64; }
+int g_hash_load_pct = 45;  // target load factor of the hash index, percent
+
+u64 hash_capacity(u64 n) { return ((n * 100 + g_hash_load_pct - 1) / g_hash_load_pct + 63) / 64 * 64; }
 
 bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s)
 {

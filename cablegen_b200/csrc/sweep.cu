@@ -61,10 +61,9 @@ struct StoreSink : LayerSink {
         // (the device query is not free: ask only when the store took a new chunk)
         if (store.chunk_count() != checked_at) {
             const u64 want = reserve_bytes + 12 * n * 8;
-            while (device_available_bytes(device) < want) {
-                if (!out->fence_main() || !CGB_CUDA(cudaStreamSynchronize(s))) return false;
-                if (!store.spill_oldest(s)) break;
-            }
+            const u64 avail = device_available_bytes(device);
+            // false when nothing is left to spill: carry on, an allocation may still fit
+            if (avail < want) store.spill(want - avail, s, out->io);
             checked_at = store.chunk_count();
         }
         return true;

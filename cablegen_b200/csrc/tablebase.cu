@@ -36,6 +36,7 @@ SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws)
 namespace cgb {
 extern int g_solve_variant;
 extern int g_sort_variant;
+extern int g_hash_load_pct;
 }
 
 static Engine &E() { return Engine::get(); }
@@ -102,6 +103,12 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         g_sort_variant = (int)value;
+    } else if (k == "hash_load_pct") {
+        if (value < 10 || value > 90) {
+            set_error("cgb_set_option: hash_load_pct must be in [10, 90]");
+            return -1;
+        }
+        g_hash_load_pct = (int)value;
     } else if (k == "spill_reserve_mb") {
         if (value < 0) {
             set_error("cgb_set_option: spill_reserve_mb must be >= 0");
@@ -140,6 +147,7 @@ long long cgb_get_option(const char *name)
     if (k == "bucket_bits") return E().bucket_bits;
     if (k == "solve_variant") return g_solve_variant;
     if (k == "sort_variant") return g_sort_variant;
+    if (k == "hash_load_pct") return g_hash_load_pct;
     if (k == "spill_reserve_mb") return (long long)(E().spill_reserve >> 20);
     if (k == "max_sort_keys") return (long long)E().max_sort_keys;
     if (k == "store_chunk_mb") return (long long)(E().store_chunk >> 20);

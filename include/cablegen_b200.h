@@ -43,7 +43,8 @@ int cgb_set_rules(const cgb_rules *rules);
  * CTAs with bulk-copy prefetch of the next tile), "spill_reserve_mb"
  * (free device memory kept before resident layers spill to host memory),
  * "max_sort_keys" (larger layer steps are cut into chunks and merged),
- * "store_chunk_mb" (device allocation unit of the resident-layer store).
+ * "store_chunk_mb" (device allocation unit of the resident-layer store),
+ * "hash_load_pct" (target load factor of the hash index, 10..90, default 45).
  * cgb_get_option returns -1 for an unknown name. */
 int cgb_set_option(const char *name, long long value);
 long long cgb_get_option(const char *name);
@@ -200,6 +201,9 @@ typedef struct {
     uint64_t h2d_bytes, d2h_bytes;
 } cgb_batch_stats;
 int cgb_batch_run(const cgb_batch *batch, cgb_batch_stats *stats);
+/* Host only: the groups cgb_batch_run would form (group_of[i] for formation i);
+ * returns the number of groups, or -1 on invalid formations. */
+int cgb_batch_plan(const cgb_formation *formations, int n_formations, int *group_of);
 
 #ifdef __cplusplus
 }

@@ -107,3 +107,40 @@ def test_batch_symmetric_masks_split_into_groups(cuda):
             assert np.array_equal(layers[(i, s)], want[s]), (i, s)
         for s in vals:
             assert np.array_equal(tables[(i, s)][1], vals[s]), (i, s)
+
+
+def test_batch_knobs_do_not_change_results(cuda, batch_case):
+    """Every tuned knob value gives the same FP64 tables (the autotuner picks speed only)."""
+    w, forms, (want_layers, want_vals) = batch_case
+    cuda.set_rules(w.settings)
+    names = ("sort_variant", "solve_variant", "hash_load_pct")
+    old = {k: cuda.get_option(k) for k in names}
+    try:
+        for sv, so, hl in ((2, 1, 60), (0, 0, 35)):
+            cuda.set_option("sort_variant", sv)
+            cuda.set_option("solve_variant", so)
+            cuda.set_option("hash_load_pct", hl)
+            _, tables, _ = cuda.batch(forms, precision=64, keep_tables=True)
+            for i in range(len(forms)):
+                for s, vals in want_vals[i].items():
+                    assert np.array_equal(tables[(i, s)][1], vals), (sv, so, hl, i, s)
+    finally:
+        for k, v in old.items():
+            cuda.set_option(k, v)
+
+
+def test_autotune_applies_and_caches(cuda, tmp_path):
+    from cablegen_b200 import autotune
+    names = tuple(autotune.KNOBS)
+    old = {k: cuda.get_option(k) for k in names}
+    try:
+        cache = str(tmp_path / "tune.json")
+        r = autotune.tune("batch64", end_cap=60, precision=32, repeats=1, cache=cache)
+        assert not r["cached"] and len(r["trials"]) == 1 + sum(len(v) - 1 for v in autotune.KNOBS.values())
+        for k, v in r["params"].items():
+            assert v in autotune.KNOBS[k] and cuda.get_option(k) == v
+        again = autotune.tune("batch64", end_cap=60, precision=32, repeats=1, cache=cache)
+        assert again["cached"] and again["params"] == r["params"]
+    finally:
+        for k, v in old.items():
+            cuda.set_option(k, v)
