@@ -69,6 +69,26 @@ def dist_env():
     return world, rank, local
 
 
+
+def aggregate_ranks(dist, boards, dev_ms, e2e=None, tensor_device="cuda"):
+    """Whole-job figures of N independent replicas: boards summed over ranks, the slowest
+    rank's device time, and (e2e = (boards, wall seconds) of this rank) the end-to-end rate
+    as all ranks' boards over the slowest rank's wall time.  Every rank makes the same
+    collective calls in the same order."""
+    import torch
+    b = torch.tensor([float(boards)], dtype=torch.float64, device=tensor_device)
+    t = torch.tensor([float(dev_ms)], dtype=torch.float64, device=tensor_device)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    rate = None
+    eb = torch.tensor([float(e2e[0]) if e2e else 0.0], dtype=torch.float64, device=tensor_device)
+    ew = torch.tensor([float(e2e[1]) if e2e else 0.0], dtype=torch.float64, device=tensor_device)
+    dist.all_reduce(eb, op=dist.ReduceOp.SUM)
+    dist.all_reduce(ew, op=dist.ReduceOp.MAX)
+    if e2e and float(ew[0]) > 0:
+        rate = float(eb[0]) / float(ew[0])
+    return float(b[0]), float(t[0]), rate
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -351,15 +371,10 @@ def run_ours(args):
 
     # ---- aggregate over ranks: sum of boards / slowest rank
     if dist is not None:
-        t = torch.tensor([boards, dev_ms, wall], dtype=torch.float64, device="cuda")
-        tb = t.clone()
-        dist.all_reduce(tb[0:1], op=dist.ReduceOp.SUM)
-        dist.all_reduce(tb[1:3], op=dist.ReduceOp.MAX)
-        boards_all, dev_ms_max = float(tb[0]), float(tb[1])
+        e2e_in = (e2e_boards, e2e_wall) if e2e is not None else None
+        boards_all, dev_ms_max, e2e_rate = aggregate_ranks(dist, boards, dev_ms, e2e_in, "cuda")
         if e2e is not None:
-            te = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
-            dist.all_reduce(te, op=dist.ReduceOp.MIN)
-            e2e["value"] = float(te[0]) * world
+            e2e["value"] = e2e_rate
     else:
         boards_all, dev_ms_max = boards, dev_ms
     value = boards_all / (dev_ms_max / 1000.0)
