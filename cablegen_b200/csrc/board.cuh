@@ -199,28 +199,31 @@ struct PruneParams {
 
 __host__ __device__ __forceinline__ bool prune_board(u64 b, const PruneParams &p)
 {
+    // one-hot bit of each tile value: values below smallest_large are small (their
+    // one-hot bit is their weight 2^e, an empty cell weighing 1), values from it up
+    // to 0xd are large.  Copies of a large value other than smallest_large pass
+    // through once/twice/thrice; smallest_large's first three copies are free, so
+    // it dies at its sixth copy.
+    const long long sl = p.smallest_large;
+    const u32 small_mask = sl <= 0 ? 0u : (sl >= 14 ? 0x3FFFu : (1u << sl) - 1u);
+    const u32 large_mask = 0x3FFFu & ~small_mask;
+    const u32 sl_bit = (sl >= 0 && sl < 14) ? (1u << sl) : 0u;
+    const u32 chain_mask = large_mask & ~sl_bit;
+    const u32 w[2] = {(u32)(b >> 32), (u32)b};
+    u32 once = 0, twice = 0, thrice = 0, small = 0;
     int large = 0, sl_count = 0;
-    long long small_sum = 0;
-    u32 once = 0, twice = 0;
-    bool dead = false;
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
-        const int e = (int)((b >> (4 * c)) & 0xF);
-        if (e >= p.smallest_large && e < 0xE) {
-            large++;
-            if (e == p.smallest_large && sl_count < 3) {
-                sl_count++;
-            } else {
-                const u32 bit = 1u << e;
-                if (twice & bit) dead = true;
-                twice |= once & bit;
-                once |= bit;
-            }
-        } else if (e < 0xE) {
-            small_sum += 1ll << e;
-        }
+    for (int k = 0; k < 16; k++) {
+        const u32 bit = 1u << ((w[k >> 3] >> (4 * (k & 7))) & 0xF);
+        small += bit & small_mask;
+        large += (bit & large_mask) != 0;
+        sl_count += bit == sl_bit;
+        const u32 c = bit & chain_mask;
+        thrice |= twice & c;
+        twice |= once & c;
+        once |= c;
     }
-    return dead || small_sum > p.stsl + 64 || large > p.ltc;
+    return thrice != 0 || sl_count >= 6 || (long long)small > p.stsl + 64 || large > p.ltc;
 }
 
 // contains tile x?  (src/generate.c:89-96 returns the negation)

@@ -113,10 +113,14 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
             if (live && !(pp.enabled && prune_board(b, pp))) {
                 u64 v[4];
                 views(b, v);
+                // a move that merges nothing keeps the multiset of tiles, so it keeps
+                // the input's (passing) prune verdict; merges show as new empty cells
+                const int empties = pp.enabled ? popc64(empty_mask(b)) : 0;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     u64 m;
-                    if (move_left(t, v[k], &m) == 2 && !(pp.enabled && prune_board(m, pp))) {
+                    if (move_left(t, v[k], &m) == 2 &&
+                        !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
                         r[k] = canonical(m);
                         mask |= 1u << k;
                     }
