@@ -13,6 +13,11 @@
 #include "../../include/cablegen_format.h"
 #include <algorithm>
 #include <cctype>
+#include <condition_variable>
+#include <deque>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <cerrno>
 #include <climits>
 #include <cstdarg>
@@ -351,18 +356,132 @@ bool write_file(const std::string &name, const void *a, u64 na, const void *b, u
     return ok;
 }
 
-// layers from the engine go straight to "<sum>.boards" files
+// Files are written by one host thread while the GPU goes on with the next
+// layers (the reference writes each layer from the layer loop itself,
+// src/generate.c:74-87, src/solve.c:29-106).  Each job waits for its
+// device-to-host copy (an event on the engine's I/O stream), writes, and hands
+// its pinned buffer back; at most `slots` jobs are in flight.
+class FileWriter {
+  public:
+    struct Job {
+        cudaEvent_t ready = nullptr;             // the copy into the buffer is complete
+        std::function<void()> write;             // runs on the writer thread
+        int slot = -1;                           // pinned buffer to hand back
+    };
+    explicit FileWriter(int slots) : stages_(slots), free_(slots, true)
+    {
+        cudaGetDevice(&device_);
+        thread_ = std::thread([this] { run(); });
+    }
+    ~FileWriter() { finish(); }
+    // a free pinned buffer of at least `bytes` (waits for the writer if none is free)
+    int take(u64 bytes, void **p)
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return std::find(free_.begin(), free_.end(), true) != free_.end(); });
+        const int i = (int)(std::find(free_.begin(), free_.end(), true) - free_.begin());
+        free_[i] = false;
+        lk.unlock();
+        if (!stages_[i].reserve(bytes + 8)) {
+            give_back(i);
+            return -1;
+        }
+        *p = stages_[i].p;
+        return i;
+    }
+    void submit(Job j)
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        jobs_.push_back(std::move(j));
+        cv_.notify_all();
+    }
+    void finish()
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            if (done_) return;
+            done_ = true;
+            cv_.notify_all();
+        }
+        thread_.join();
+    }
+
+  private:
+    std::vector<cgb::HostStage> stages_;
+    std::vector<bool> free_;
+    std::deque<Job> jobs_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    bool done_ = false;
+    int device_ = 0;
+    std::thread thread_;
+
+    void give_back(int i)
+    {
+        std::lock_guard<std::mutex> lk(m_);
+        free_[i] = true;
+        cv_.notify_all();
+    }
+    void run()
+    {
+        cudaSetDevice(device_);
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return done_ || !jobs_.empty(); });
+                if (jobs_.empty()) return;
+                j = std::move(jobs_.front());
+                jobs_.pop_front();
+            }
+            if (j.ready) {
+                CGB_CUDA(cudaEventSynchronize(j.ready));
+                cudaEventDestroy(j.ready);
+            }
+            j.write();
+            if (j.slot >= 0) give_back(j.slot);
+        }
+    }
+};
+
+// an event on `main` that `io` waits for, then a copy on `io` and its completion event
+cudaEvent_t copy_on_io(void *dst, const void *src, u64 bytes, cudaStream_t main, cudaStream_t io)
+{
+    cudaEvent_t before = nullptr, after = nullptr;
+    if (!CGB_CUDA(cudaEventCreateWithFlags(&before, cudaEventDisableTiming)) ||
+        !CGB_CUDA(cudaEventCreateWithFlags(&after, cudaEventDisableTiming)))
+        return nullptr;
+    bool ok = CGB_CUDA(cudaEventRecord(before, main)) && CGB_CUDA(cudaStreamWaitEvent(io, before, 0)) &&
+              (bytes == 0 || CGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, io))) &&
+              CGB_CUDA(cudaEventRecord(after, io));
+    cudaEventDestroy(before);
+    if (!ok) {
+        cudaEventDestroy(after);
+        return nullptr;
+    }
+    return after;
+}
+
+// layers from the engine go to "<sum>.boards" files through the writer
 struct FileSink : cgb::LayerSink {
-    const char *fmt;
-    cgb::HostStage stage;
+    const char *fmt = nullptr;
+    FileWriter *writer = nullptr;
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
         *kept = false;
-        if (!stage.reserve(n * 8 + 8)) return false;
-        if (n && !CGB_CUDA(cudaMemcpyAsync(stage.p, d, n * 8, cudaMemcpyDeviceToHost, s))) return false;
-        if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
-        static_arr_info a{true, (uint64_t *)stage.p, (size_t)n};
-        write_boards(a, fmt, sum);
+        void *h = nullptr;
+        const int slot = writer->take(n * 8, &h);
+        if (slot < 0) return false;
+        // the engine reuses its layer buffer: the copy must be done before the
+        // main stream goes on, so it waits for the I/O stream's event
+        cudaEvent_t ev = copy_on_io(h, d, n * 8, s, cgb::Engine::get().io_stream);
+        if (!ev || !CGB_CUDA(cudaStreamWaitEvent(s, ev, 0))) return false;
+        const std::string f = fmt;
+        writer->submit({ev, [h, n, f, sum] {
+                            static_arr_info a{true, (uint64_t *)h, (size_t)n};
+                            write_boards(a, f.c_str(), sum);
+                        },
+                        slot});
         return true;
     }
 };
@@ -617,10 +736,14 @@ void generate(const int start, const int end, const char *fmt, const static_arr_
     generate_lut();
     if (s.premove) logf(L_WARN, "premove is not supported (the reference's premove path is broken); ignoring it");
     if (!engine_ready()) die("generate: GPU engine");
+    FileWriter writer(3);
     FileSink sink;
     sink.fmt = fmt;
+    sink.writer = &writer;
     cgb::GenTimes tm;
-    if (!cgb::Engine::get().generate(initial->bp, initial->size, start, end, sink, &tm)) die("generate");
+    const bool ok = cgb::Engine::get().generate(initial->bp, initial->size, start, end, sink, &tm);
+    writer.finish();
+    if (!ok) die("generate");
     rusage ru;
     if (getrusage(RUSAGE_SELF, &ru) == 0) logf(L_INFO, "Peak host RSS:  %.2f MiB", ru.ru_maxrss / 1024.0);
 }
@@ -648,8 +771,7 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
         cgb::LayerIndex ix;
     };
     Lay t2, t4, cur;
-    cgb::HostStage hs;
-    std::vector<double> widened;
+    FileWriter writer(3);
     for (unsigned i = start; i >= end && i; i -= 2) {
         const std::string bname = fmt_layer(posfmt, i);
         static_arr_info keys = read_boards(bname.c_str());
@@ -665,29 +787,46 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
                                 : cgb::solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, rules, e.rt,
                                                         e.ctr, st);
         if (!ok) die("solve");
-        if (!hs.reserve(cur.n * vb + 8)) die("solve");
-        if (cur.n && !CGB_CUDA(cudaMemcpyAsync(hs.p, cur.vals, cur.n * vb, cudaMemcpyDeviceToHost, st))) die("solve");
-        if (!CGB_CUDA(cudaStreamSynchronize(st))) die("solve");
-        const void *vals = hs.p;
-        if (vb == 4) {  // FP32 tables are written as f64, as the file format demands
-            widened.resize(cur.n);
-            for (u64 k = 0; k < cur.n; k++) widened[k] = ((const float *)hs.p)[k];
-            vals = widened.data();
-        }
+        // the values go to a pinned buffer on the I/O stream; the writer thread
+        // writes the table (keys from the .boards file, values widened to f64
+        // for FP32 tables, as the file format demands) while the next layer runs
+        void *h = nullptr;
+        const int slot = writer.take(cur.n * vb, &h);
+        if (slot < 0) die("solve");
+        cudaEvent_t ev = copy_on_io(h, cur.vals, cur.n * vb, st, e.io_stream);
+        if (!ev) die("solve");
         const std::string tname = fmt_layer(tablefmt, i);
-        logf(L_INFO, "Writing %lu boards to %s (%lu bytes)", (unsigned long)cur.n, tname.c_str(),
-             (unsigned long)(16 * cur.n));
-        write_file(tname, keys.bp, 8 * cur.n, vals, 8 * cur.n);
-        print_speed(cur.n);
-        std::free(keys.bp);
+        const u64 n = cur.n;
+        writer.submit({ev, [tname, keys, h, n, vb] {
+                           const void *vals = h;
+                           std::vector<double> widened;
+                           if (vb == 4) {
+                               widened.resize(n);
+                               for (u64 k = 0; k < n; k++) widened[k] = ((const float *)h)[k];
+                               vals = widened.data();
+                           }
+                           logf(L_INFO, "Writing %lu boards to %s (%lu bytes)", (unsigned long)n, tname.c_str(),
+                                (unsigned long)(16 * n));
+                           write_file(tname, keys.bp, 8 * n, vals, 8 * n);
+                           print_speed(n);
+                           std::free(keys.bp);
+                       },
+                       slot});
         cur.ix.keys = cur.keys;
         cur.ix.vals = cur.vals;
         cur.ix.n = cur.n;
         if (!cgb::build_index(cur.ix, e.index_kind, vb, cur.store, e.bucket_bits, e.ctr, st)) die("solve");
+        // the I/O stream may still read t4's values: free after its copies
+        cudaEvent_t io_done = nullptr;
+        if (!CGB_CUDA(cudaEventCreateWithFlags(&io_done, cudaEventDisableTiming)) ||
+            !CGB_CUDA(cudaEventRecord(io_done, e.io_stream)) || !CGB_CUDA(cudaStreamWaitEvent(st, io_done, 0)))
+            die("solve");
+        cudaEventDestroy(io_done);
         for (void *p : {(void *)t4.keys, t4.vals, t4.store.p}) cgb::dev_free(p, st);
         t4 = t2;
         t2 = cur;
     }
+    writer.finish();
     for (Lay *x : {&t2, &t4})
         for (void *p : {(void *)x->keys, x->vals, x->store.p}) cgb::dev_free(p, st);
     cgb::dev_free(d_ws, st);
