@@ -43,6 +43,12 @@ METRIC = "Boards/s gen+solve, FP32 vs FP64 solve at <=1e-6 err; lookup/sort HBM 
 REF_CLI = os.path.join(ROOT, "oracle", "_ref", "cli")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per unit of work from the ncu captures summarised in profiles/
+# (smaller cases of the same kernels; their traffic grows in proportion to the units):
+# a sort digit pass per key (onesweep_sort_88M_ll_keys.md), the solve per board
+# (solve_f64_hash_ll_end260.md), the move expansion per input board (expand_moves_30M_ll_boards.md).
+NCU_DRAM_BYTES_PER_UNIT = {"onesweep": 1.398311e9 / 88333334, "solve": 3.308543e9 / 7822359,
+                           "expand": 579.8e6 / 30e6}
 
 
 def parse():
@@ -386,9 +392,19 @@ def run_ours(args):
             "hist": "sort histogram"}
     dom = max(fams, key=lambda k: kst[f"{k}_ms"])
     achieved = kst[f"{dom}_bytes"] / 1e9 / (kst[f"{dom}_ms"] / 1000.0) if kst[f"{dom}_ms"] else 0.0
+    # traffic of the dominant kernel per launch: ncu bytes per unit x the mean units per launch
+    traffic, traffic_note = None, None
+    units = {"onesweep": (kst["onesweep_bytes"] / 16.0, kst["onesweep_launches"], "keys per pass"),
+             "solve": (kst["solve_boards"], kst["solve_launches"], "boards")}
+    if dom in units and dom in NCU_DRAM_BYTES_PER_UNIT and units[dom][1]:
+        per_launch_units = units[dom][0] / units[dom][1]
+        traffic = NCU_DRAM_BYTES_PER_UNIT[dom] * per_launch_units / 1e9
+        traffic_note = (f"GB per launch: ncu DRAM bytes per unit ({NCU_DRAM_BYTES_PER_UNIT[dom]:.2f}) x mean "
+                        f"{units[dom][2]} per launch ({per_launch_units:.0f}); algorithmic GB per launch "
+                        f"{kst[dom + '_bytes'] / units[dom][1] / 1e9:.4f}")
     roofline = {"kernel": fams[dom], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
-                "traffic": None,
+                "traffic": traffic, "traffic_note": traffic_note,
                 "kernels": {k: {"ms": round(kst[f"{k}_ms"], 3),
                                 "GB/s": round(kst[f"{k}_bytes"] / 1e6 / kst[f"{k}_ms"], 1) if kst[f"{k}_ms"] else None,
                                 "share": round(kst[f"{k}_ms"] / max(dev_ms, 1e-9), 4)}
