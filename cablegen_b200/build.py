@@ -76,6 +76,30 @@ def build(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
+CL_LIB = os.path.join(HERE, "libcablegen_b200_cl.so")
+
+
+def build_cl_seam(verbose: bool = False) -> str:
+    """libcablegen_b200_cl.so: the reference's GPU plug-in seam (include/cablegen_cl.h) on the
+    engine, without the library's own restatement of the reference API (refapi.cu), so the
+    reference's own objects can link it; their get_settings_min() is resolved at load time."""
+    build(verbose)
+    hdr_mtime = max([os.path.getmtime(h) for h in _headers()] + [os.path.getmtime(__file__)])
+    seam = _compile(os.path.join(CSRC, "clseam", "cl_seam.cu"), hdr_mtime, verbose)
+    objs = [os.path.join(OUT_DIR, os.path.basename(s) + ".o") for s in _sources()
+            if os.path.basename(s) not in ("refapi.cu",)] + [seam]
+    newest = max(os.path.getmtime(o) for o in objs)
+    if not os.path.exists(CL_LIB) or os.path.getmtime(CL_LIB) < newest:
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", CL_LIB + ".tmp"] + objs + ["-lcudart_static", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(CL_LIB + ".tmp", CL_LIB)
+    return CL_LIB
+
+
 CLI = os.path.join(OUT_DIR, "cli_b200")
 
 

@@ -61,9 +61,9 @@ def lib(tmp_path_factory):
     return L
 
 
-def declared_functions():
+def declared_functions(headers=HEADERS):
     names = set()
-    for h in HEADERS:
+    for h in headers:
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\([^;{]*\)\s*;", text, flags=re.M):
@@ -79,6 +79,21 @@ def test_every_declared_symbol_is_exported():
             "format_str"} <= names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
+
+
+def test_cl_seam_exports_every_declared_function():
+    """libcablegen_b200_cl.so (the reference's GPU plug-in seam on this engine) defines every
+    cl_* function of include/cablegen_cl.h and leaves only get_settings_min() to the reference's
+    objects it is linked with."""
+    import subprocess
+    lib = os.path.join(ROOT, "cablegen_b200", "libcablegen_b200_cl.so")
+    names = declared_functions([os.path.join(ROOT, "include", "cablegen_cl.h")])
+    assert len(names) == 11 and all(n.startswith("cl_") for n in names), names
+    out = subprocess.run(["nm", "-D", lib], capture_output=True, text=True, check=True).stdout
+    defined = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    undefined = {l.split()[-1] for l in out.splitlines() if l.split()[0] == "U" and "@" not in l}
+    assert names <= defined, names - defined
+    assert undefined == {"get_settings_min"}, undefined
 
 
 @pytest.mark.parametrize("ff,ig", [(0, 0), (0, 1), (1, 0), (1, 1)])
