@@ -403,7 +403,9 @@ def run_ours(args):
                         f"{units[dom][2]} per launch ({per_launch_units:.0f}); algorithmic GB per launch "
                         f"{kst[dom + '_bytes'] / units[dom][1] / 1e9:.4f}")
     roofline = {"kernel": fams[dom], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                "frac": achieved / peak, "peak_source": ("measured hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else
+                                "fallback: the profiling recipe's earlier measurement on this pool "
+                                "(MEASURED_PEAKS.json absent)"),
                 "traffic": traffic, "traffic_note": traffic_note,
                 "kernels": {k: {"ms": round(kst[f"{k}_ms"], 3),
                                 "GB/s": round(kst[f"{k}_bytes"] / 1e6 / kst[f"{k}_ms"], 1) if kst[f"{k}_ms"] else None,
