@@ -344,6 +344,7 @@ bool run_group(Engine &e, const cgb_batch *b, std::vector<Plan> &plans, cgb_batc
         kstats().launches += 2;
         st->boards_solved += n;
         st->solve_steps++;
+        const bool enqueued = b->table_fn != nullptr;  // this step's copy reads only cur
         if (b->table_fn) {
             // one copy of the step's union; the callback hands out each formation's range
             // (formations whose layer is empty at this step get an empty table)
@@ -369,8 +370,9 @@ bool run_group(Engine &e, const cgb_batch *b, std::vector<Plan> &plans, cgb_batc
                              });
             if (!ok) break;
         }
-        // blocks whose every range has been gathered leave the store
-        ok = out.fence_main();
+        // blocks whose every range has been gathered leave the store (the copy
+        // just enqueued reads cur, not them)
+        ok = out.fence_main(enqueued);
         for (auto &x : srcs) {
             auto &blk = sink.blocks[x.second.block];
             if (--blk.refs == 0 && blk.live) {

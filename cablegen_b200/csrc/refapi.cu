@@ -793,6 +793,12 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
         void *h = nullptr;
         const int slot = writer.take(cur.n * vb, &h);
         if (slot < 0) die("solve");
+        // copies of the earlier layers (t4's values among them) end at this
+        // event; the copy of this layer's values, enqueued next, is not waited for
+        cudaEvent_t earlier_io = nullptr;
+        if (!CGB_CUDA(cudaEventCreateWithFlags(&earlier_io, cudaEventDisableTiming)) ||
+            !CGB_CUDA(cudaEventRecord(earlier_io, e.io_stream)))
+            die("solve");
         cudaEvent_t ev = copy_on_io(h, cur.vals, cur.n * vb, st, e.io_stream);
         if (!ev) die("solve");
         const std::string tname = fmt_layer(tablefmt, i);
@@ -816,12 +822,9 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
         cur.ix.vals = cur.vals;
         cur.ix.n = cur.n;
         if (!cgb::build_index(cur.ix, e.index_kind, vb, cur.store, e.bucket_bits, e.ctr, st)) die("solve");
-        // the I/O stream may still read t4's values: free after its copies
-        cudaEvent_t io_done = nullptr;
-        if (!CGB_CUDA(cudaEventCreateWithFlags(&io_done, cudaEventDisableTiming)) ||
-            !CGB_CUDA(cudaEventRecord(io_done, e.io_stream)) || !CGB_CUDA(cudaStreamWaitEvent(st, io_done, 0)))
-            die("solve");
-        cudaEventDestroy(io_done);
+        // the I/O stream may still read t4's values (copied two layers ago)
+        if (!CGB_CUDA(cudaStreamWaitEvent(st, earlier_io, 0))) die("solve");
+        cudaEventDestroy(earlier_io);
         for (void *p : {(void *)t4.keys, t4.vals, t4.store.p}) cgb::dev_free(p, st);
         t4 = t2;
         t2 = cur;

@@ -227,7 +227,9 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
                 break;
             }
         }
+        bool enqueued = false;  // this layer's table copy (reads only this layer)
         if (w->table_fn) {
+            enqueued = true;
             Chain &c = chains[0];
             const int prec = c.vbytes == 8 ? 64 : 32;
             cgb_table_fn f = w->table_fn;
@@ -239,8 +241,10 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         }
         for (auto &c : chains) ok = ok && c.index(e, s);
         if (!ok) break;
-        // the s+4 layer is no longer needed by anyone
-        ok = out.fence_main();
+        // the s+4 layer is no longer needed by anyone; its copies went out two
+        // layers ago (the copy just enqueued reads only this layer, so the main
+        // stream goes on without waiting for it)
+        ok = out.fence_main(enqueued);
         const int gone = chains[0].t4.sum;
         for (auto &c : chains) c.rotate(s);
         auto it4 = by_sum.find(gone);
