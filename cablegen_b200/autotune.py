@@ -6,8 +6,9 @@ The knobs (cgb_set_option):
   match, 1 with eight ballots per digit (keys re-read from L2 for the local scatter), 2 keeps
   persistent CTAs that bulk-copy the next tile into shared memory while ranking the current one;
 * ``solve_variant`` -- 0 one thread per board, 1 warp-compacted successor queue;
-* ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (slots per
-  key: fewer means more probes, more means more memory and a lower L2 hit rate).
+* ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
+  table size; a higher load means more probes, a lower one more memory and a lower L2 hit
+  rate).
 
 The digit width stays at 8 bits: the look-back words and the per-tile histograms grow with the
 radix (2048 bins at 11 bits), which costs more than the pass it saves on 48 varying key bits.
@@ -28,7 +29,7 @@ from . import configs, device
 KNOBS = {
     "sort_variant": [1, 0, 2],
     "solve_variant": [0, 1],
-    "hash_load_pct": [45, 35, 60],
+    "hash_load_pct": [0, 25, 45],
 }
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "cablegen_b200", "autotune.json")

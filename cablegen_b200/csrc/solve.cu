@@ -589,9 +589,16 @@ bool solve_layer_enqueue(const u64 *keys, u64 n, void *out, int vbytes, const La
 
 bool solve_prepare() { return solve_attrs(); }
 
-int g_hash_load_pct = 45;  // target load factor of the hash index, percent
+// target load factor of the hash index, percent; 0 = by size: 25 % (64 bytes
+// of slots per board: fewer probes, measured 10 % faster solve + build on LL
+// layers than 45 %) up to 2^27 keys, 45 % above, where table memory counts
+int g_hash_load_pct = 0;
 
-u64 hash_capacity(u64 n) { return ((n * 100 + g_hash_load_pct - 1) / g_hash_load_pct + 63) / 64 * 64; }
+u64 hash_capacity(u64 n)
+{
+    const u64 pct = g_hash_load_pct ? (u64)g_hash_load_pct : (n <= (1ull << 27) ? 25 : 45);
+    return ((n * 100 + pct - 1) / pct + 63) / 64 * 64;
+}
 
 bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s)
 {

@@ -104,8 +104,8 @@ int cgb_set_option(const char *name, long long value)
         }
         g_sort_variant = (int)value;
     } else if (k == "hash_load_pct") {
-        if (value < 10 || value > 90) {
-            set_error("cgb_set_option: hash_load_pct must be in [10, 90]");
+        if (value != 0 && (value < 10 || value > 90)) {
+            set_error("cgb_set_option: hash_load_pct must be 0 (by size) or in [10, 90]");
             return -1;
         }
         g_hash_load_pct = (int)value;
