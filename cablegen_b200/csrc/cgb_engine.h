@@ -107,7 +107,11 @@ struct Engine {
     bool spawn_layer(GenTimes *tm);
     bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm);
     bool merge_into(DevBuf<u64> &acc, const u64 *run, u64 n);
-    bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm);
+    // layers start..end from the input set of layer `start`; h_carry = the
+    // 4-spawns of layer start-2 still to merge into layer start+2's input
+    // (empty for a fresh sweep, the checkpointed set when resuming)
+    bool generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm,
+                  const u64 *h_carry = nullptr, u64 n_carry = 0);
     void release_buffers();
 };
 

@@ -434,14 +434,16 @@ bool Engine::spawn_layer(GenTimes *tm)
     return true;
 }
 
-bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm)
+bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, LayerSink &sink, GenTimes *tm,
+                      const u64 *h_carry, u64 n_carry)
 {
     cudaStream_t s = stream;
     GenBuffers &g = gen;
-    if (!reserve(g.S, n_init, s)) return false;
+    if (!reserve(g.S, n_init, s) || !reserve(g.u4, n_carry, s)) return false;
     if (n_init && !CGB_CUDA(cudaMemcpyAsync(g.S.p, h_initial, n_init * 8, cudaMemcpyHostToDevice, s))) return false;
+    if (n_carry && !CGB_CUDA(cudaMemcpyAsync(g.u4.p, h_carry, n_carry * 8, cudaMemcpyHostToDevice, s))) return false;
     g.S.n = n_init;
-    g.u4.n = 0;
+    g.u4.n = n_carry;
     bool ok = true;
     for (int layer = start; layer <= end && ok; layer += 2) {
         ok = move_layer(g.S.p, g.S.n, tm);

@@ -70,6 +70,10 @@ struct Settings {
     bool prune;
     bool score;
     bool fp32;  // [Solve] fp32: solve with FP32 tables (library extension, default off)
+    // [Generate] checkpoint / resume (library extension, default off): write, after
+    // each layer, the state the next layer starts from; start from the newest one
+    bool checkpoint;
+    bool resume;
 };
 
 Settings g_settings = [] {
@@ -97,6 +101,8 @@ Settings g_settings = [] {
     s.prune = false;
     s.score = false;
     s.fp32 = false;
+    s.checkpoint = false;
+    s.resume = false;
     return s;
 }();
 bool g_settings_read = false;
@@ -209,6 +215,8 @@ void read_settings()
     i("Generate", "ltc", &s.ltc);
     i("Generate", "smallest_large", &s.smallest_large);
     b("Generate", "prune", &s.prune);
+    b("Generate", "checkpoint", &s.checkpoint);
+    b("Generate", "resume", &s.resume);
     str("Solve", "dir", &s.min.tdir);
     str("Solve", "winstates", &s.min.winstates);
     i("Solve", "end", &s.min.end_solve);
@@ -462,19 +470,30 @@ cudaEvent_t copy_on_io(void *dst, const void *src, u64 bytes, cudaStream_t main,
     return after;
 }
 
+// Resume point of a generation: after layer s the engine holds the input set
+// of layer s+2 and the 4-spawns of layer s that join layer s+4's input.  A
+// checkpoint file "<layer s+2 file>.resume" stores them: four u64 words
+// {CKPT_MAGIC, s + 2, |input|, |carry|}, then the two sorted arrays.
+constexpr uint64_t CKPT_MAGIC = 0x31454d5553455247ull;  // "GRESUME1"
+
+std::string checkpoint_name(const char *fmt, int next) { return fmt_layer(fmt, next) + ".resume"; }
+
 // layers from the engine go to "<sum>.boards" files through the writer
 struct FileSink : cgb::LayerSink {
     const char *fmt = nullptr;
     FileWriter *writer = nullptr;
+    bool checkpoint = false;
+    std::string last_checkpoint;  // written by the writer thread, removed when superseded
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
         *kept = false;
+        cgb::Engine &e = cgb::Engine::get();
         void *h = nullptr;
         const int slot = writer->take(n * 8, &h);
         if (slot < 0) return false;
         // the engine reuses its layer buffer: the copy must be done before the
         // main stream goes on, so it waits for the I/O stream's event
-        cudaEvent_t ev = copy_on_io(h, d, n * 8, s, cgb::Engine::get().io_stream);
+        cudaEvent_t ev = copy_on_io(h, d, n * 8, s, e.io_stream);
         if (!ev || !CGB_CUDA(cudaStreamWaitEvent(s, ev, 0))) return false;
         const std::string f = fmt;
         writer->submit({ev, [h, n, f, sum] {
@@ -482,9 +501,76 @@ struct FileSink : cgb::LayerSink {
                             write_boards(a, f.c_str(), sum);
                         },
                         slot});
+        if (checkpoint && !write_checkpoint(sum + 2, s)) return false;
+        return true;
+    }
+    bool write_checkpoint(int next, cudaStream_t s)
+    {
+        cgb::Engine &e = cgb::Engine::get();
+        const u64 ns = e.gen.S.n, nc = e.gen.u4.n;
+        void *h = nullptr;
+        const int slot = writer->take(8 * (4 + ns + nc), &h);
+        if (slot < 0) return false;
+        uint64_t *w = (uint64_t *)h;
+        w[0] = CKPT_MAGIC;
+        w[1] = (uint64_t)next;
+        w[2] = ns;
+        w[3] = nc;
+        cudaEvent_t before = nullptr;
+        if (!CGB_CUDA(cudaEventCreateWithFlags(&before, cudaEventDisableTiming)) ||
+            !CGB_CUDA(cudaEventRecord(before, s)) || !CGB_CUDA(cudaStreamWaitEvent(e.io_stream, before, 0)))
+            return false;
+        cudaEventDestroy(before);
+        if (ns && !CGB_CUDA(cudaMemcpyAsync(w + 4, e.gen.S.p, ns * 8, cudaMemcpyDeviceToHost, e.io_stream)))
+            return false;
+        cudaEvent_t ev = copy_on_io(w + 4 + ns, e.gen.u4.p, nc * 8, s, e.io_stream);
+        if (!ev || !CGB_CUDA(cudaStreamWaitEvent(s, ev, 0))) return false;
+        const std::string name = checkpoint_name(fmt, next), prev = last_checkpoint;
+        last_checkpoint = name;
+        const u64 bytes = 8 * (4 + ns + nc);
+        writer->submit({ev, [w, bytes, name, prev] {
+                            const std::string tmp = name + ".tmp";
+                            if (write_file(tmp, w, bytes, nullptr, 0) && std::rename(tmp.c_str(), name.c_str()) == 0) {
+                                if (!prev.empty()) std::remove(prev.c_str());
+                            } else {
+                                logf(L_WARN, "Couldn't write the checkpoint %s!", name.c_str());
+                            }
+                        },
+                        slot});
         return true;
     }
 };
+
+// the newest checkpoint of `fmt` after layer `start` (next = 0 when none; next
+// > end when the generation up to `end` is complete)
+struct Checkpoint {
+    int next = 0;
+    std::vector<u64> input, carry;
+};
+Checkpoint find_checkpoint(const char *fmt, int start, int end)
+{
+    Checkpoint c;
+    for (int next = end + 2; next > start; next -= 2) {
+        const std::string name = checkpoint_name(fmt, next);
+        FILE *f = std::fopen(name.c_str(), "rb");
+        if (!f) continue;
+        uint64_t hdr[4];
+        bool ok = std::fread(hdr, 8, 4, f) == 4 && hdr[0] == CKPT_MAGIC && hdr[1] == (uint64_t)next;
+        if (ok) {
+            c.input.resize(hdr[2]);
+            c.carry.resize(hdr[3]);
+            ok = std::fread(c.input.data(), 8, hdr[2], f) == hdr[2] && std::fread(c.carry.data(), 8, hdr[3], f) == hdr[3];
+        }
+        std::fclose(f);
+        if (ok) {
+            c.next = next;
+            return c;
+        }
+        logf(L_WARN, "Ignoring the unreadable checkpoint %s", name.c_str());
+        c = Checkpoint{};
+    }
+    return c;
+}
 
 }  // namespace
 
@@ -740,8 +826,21 @@ void generate(const int start, const int end, const char *fmt, const static_arr_
     FileSink sink;
     sink.fmt = fmt;
     sink.writer = &writer;
+    sink.checkpoint = s.checkpoint;
     cgb::GenTimes tm;
-    const bool ok = cgb::Engine::get().generate(initial->bp, initial->size, start, end, sink, &tm);
+    Checkpoint ck;
+    if (s.resume) ck = find_checkpoint(fmt, start, end);
+    bool ok = true;
+    if (ck.next > end) {
+        logf(L_INFO, "%s: every layer up to %d is already generated", checkpoint_name(fmt, ck.next).c_str(), end);
+    } else if (ck.next) {
+        logf(L_INFO, "Resuming at layer %d from %s", ck.next, checkpoint_name(fmt, ck.next).c_str());
+        sink.last_checkpoint = checkpoint_name(fmt, ck.next);
+        ok = cgb::Engine::get().generate(ck.input.data(), ck.input.size(), ck.next, end, sink, &tm, ck.carry.data(),
+                                         ck.carry.size());
+    } else {
+        ok = cgb::Engine::get().generate(initial->bp, initial->size, start, end, sink, &tm);
+    }
     writer.finish();
     if (!ok) die("generate");
     rusage ru;

@@ -54,3 +54,38 @@ def test_cli_self_test(cli_dir):
     r = subprocess.run([CLI, f"-C={conf}", "test"], cwd=work, env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "All tests passed!" in r.stdout
+
+
+def test_cli_generate_resumes_from_checkpoint(tmp_path):
+    """[Generate] checkpoint / resume (library extension): a generation stopped at tile sum 40
+    and resumed up to 60 writes the same layer files as the reference."""
+    if not os.path.exists(CLI):
+        pytest.skip("cli_b200 is built only where the reference CLI sources exist")
+    from make_golden import prepare
+    work = str(tmp_path)
+    wl, form, conf, bdir, tdir = prepare("ll_pruned", 40, work, 2)
+    with open(conf) as f:
+        text = f.read().replace("prune = true", "prune = true\ncheckpoint = true\nresume = true")
+    env = dict(os.environ, XDG_CONFIG_HOME=work)
+
+    def run(end):
+        with open(conf, "w") as f:
+            f.write(text.replace("end = 40", f"end = {end}", 1))
+        r = subprocess.run([CLI, f"-C={conf}", "generate"], cwd=work, env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        return r.stdout + r.stderr
+
+    first = run(40)
+    assert "Resuming" not in first
+    assert os.path.exists(os.path.join(bdir, "42.boards.resume"))
+    for s in range(42, 61, 2):
+        assert not os.path.exists(os.path.join(bdir, f"{s}.boards"))
+    second = run(60)
+    assert "Resuming at layer 42" in second
+    assert os.path.exists(os.path.join(bdir, "62.boards.resume"))
+    assert not os.path.exists(os.path.join(bdir, "42.boards.resume"))
+    want = digests("ll_pruned")["layers"]
+    for s in range(16, 61, 2):
+        assert sha(os.path.join(bdir, f"{s}.boards")) == want[str(s)]["boards_sha256"], s
+    assert "already generated" in run(60)
