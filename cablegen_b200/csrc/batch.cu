@@ -370,9 +370,11 @@ bool run_group(Engine &e, const cgb_batch *b, std::vector<Plan> &plans, cgb_batc
                              });
             if (!ok) break;
         }
-        // blocks whose every range has been gathered leave the store (the copy
-        // just enqueued reads cur, not them)
-        ok = out.fence_main(enqueued);
+        // blocks whose every range has been gathered leave the store, t4 below.
+        // When this step's table was enqueued, the copies still in flight are
+        // this step's and the previous step's (an enqueue first completes the
+        // copy it replaces), neither reading them; otherwise fence every copy
+        if (!enqueued) ok = out.fence_main();
         for (auto &x : srcs) {
             auto &blk = sink.blocks[x.second.block];
             if (--blk.refs == 0 && blk.live) {

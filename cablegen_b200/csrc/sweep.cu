@@ -241,10 +241,12 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         }
         for (auto &c : chains) ok = ok && c.index(e, s);
         if (!ok) break;
-        // the s+4 layer is no longer needed by anyone; its copies went out two
-        // layers ago (the copy just enqueued reads only this layer, so the main
-        // stream goes on without waiting for it)
-        ok = out.fence_main(enqueued);
+        // the s+4 layer is no longer needed by anyone.  When this layer's table
+        // was enqueued, the copies still in flight are this layer's and the
+        // previous one's (an enqueue first completes the copy it replaces, two
+        // layers back), so none reads s+4 and the main stream need not wait;
+        // otherwise fence every pending copy (layer copies of the generation)
+        if (!enqueued) ok = out.fence_main();
         const int gone = chains[0].t4.sum;
         for (auto &c : chains) c.rotate(s);
         auto it4 = by_sum.find(gone);
