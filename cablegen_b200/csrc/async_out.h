@@ -23,7 +23,6 @@ struct AsyncOut {
     };
     Slot slot[2];
     int next = 0;
-    int latest = -1;  // slot of the last enqueue
     u64 d2h = 0;
     bool failed = false;
 
@@ -62,7 +61,6 @@ struct AsyncOut {
     bool enqueue(const std::vector<std::pair<const void *, u64>> &segs, std::function<bool(const char *)> cb)
     {
         Slot &s = slot[next];
-        latest = next;
         next ^= 1;
         if (!finish(s)) return false;
         u64 bytes = 16;
@@ -83,15 +81,11 @@ struct AsyncOut {
         s.busy = true;
         return true;
     }
-    // later frees on the main stream must not overtake copies still reading;
-    // skip_latest leaves out the copy just enqueued, when the caller frees
-    // nothing that copy reads (the main stream then need not wait for it)
-    bool fence_main(bool skip_latest = false)
+    // later frees on the main stream must not overtake copies still reading
+    bool fence_main()
     {
-        for (int i = 0; i < 2; i++)
-            if (slot[i].busy && !(skip_latest && i == latest) &&
-                !CGB_CUDA(cudaStreamWaitEvent(main, slot[i].done, 0)))
-                return false;
+        for (auto &s : slot)
+            if (s.busy && !CGB_CUDA(cudaStreamWaitEvent(main, s.done, 0))) return false;
         return true;
     }
     bool drain() { return finish(slot[next]) && finish(slot[next ^ 1]); }
