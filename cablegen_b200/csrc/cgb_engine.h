@@ -70,6 +70,44 @@ struct HostStage {
     }
 };
 
+// Pinned host memory handed out in order and reset per sweep; its chunks are
+// kept, so later sweeps pin nothing new.  Holds the host copies of a sweep's
+// layers when the caller wants layers and tables both.
+struct HostArena {
+    struct Chunk {
+        void *p = nullptr;
+        u64 bytes = 0, top = 0;
+    };
+    std::vector<Chunk> chunks;
+    size_t cur = 0;
+    u64 used = 0;  // bytes handed out since the last reset
+    void *take(u64 bytes)
+    {
+        bytes = (bytes + 15) & ~15ull;
+        while (cur < chunks.size() && chunks[cur].top + bytes > chunks[cur].bytes) cur++;
+        if (cur == chunks.size()) {
+            Chunk c;
+            c.bytes = bytes > (1ull << 30) ? bytes : (1ull << 30);
+            if (cudaMallocHost(&c.p, c.bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            chunks.push_back(c);
+        }
+        Chunk &c = chunks[cur];
+        void *r = (char *)c.p + c.top;
+        c.top += bytes;
+        used += bytes;
+        return r;
+    }
+    void reset()
+    {
+        for (auto &c : chunks) c.top = 0;
+        cur = 0;
+        used = 0;
+    }
+};
+
 // working buffers of the generation sweep, kept between layers and calls
 struct GenBuffers {
     DevBuf<u64> a, b;          // raw move output and its sort scratch
@@ -103,6 +141,8 @@ struct Engine {
 
     GenBuffers gen;
     HostStage out_stage[2];     // pinned double buffer of the sweep's host copies
+    HostArena host_layers;      // host copies of a sweep's layers (layers and tables both wanted)
+    u64 host_layers_cap = 64ull << 30;  // bytes; beyond it tables carry their own key copy
     bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
     bool spawn_layer(GenTimes *tm);
     bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm);

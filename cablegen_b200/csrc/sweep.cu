@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <functional>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <vector>
 
@@ -26,7 +27,27 @@ struct Layer {
     int sum;
     LayerStore::Handle h;
     bool live;
+    const u64 *host = nullptr;  // host copy of the keys (host_layers), when kept
 };
+
+// device -> host copy on the I/O stream after the main stream's work so far;
+// returns the event that marks its completion
+cudaEvent_t copy_to_host(void *dst, const void *src, u64 bytes, cudaStream_t main, cudaStream_t io)
+{
+    cudaEvent_t before = nullptr, after = nullptr;
+    if (!CGB_CUDA(cudaEventCreateWithFlags(&before, cudaEventDisableTiming)) ||
+        !CGB_CUDA(cudaEventCreateWithFlags(&after, cudaEventDisableTiming)))
+        return nullptr;
+    const bool ok = CGB_CUDA(cudaEventRecord(before, main)) && CGB_CUDA(cudaStreamWaitEvent(io, before, 0)) &&
+                    (bytes == 0 || CGB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, io))) &&
+                    CGB_CUDA(cudaEventRecord(after, io));
+    cudaEventDestroy(before);
+    if (!ok) {
+        cudaEventDestroy(after);
+        return nullptr;
+    }
+    return after;
+}
 
 struct StoreSink : LayerSink {
     std::vector<Layer> layers;
@@ -37,6 +58,27 @@ struct StoreSink : LayerSink {
     u64 reserve_bytes = 0;
     size_t checked_at = 0;  // store chunks at the last free-memory check
     int device = 0;
+    HostArena *host = nullptr;  // set when layers and tables both go to the host
+    u64 host_cap = 0;
+    u64 host_d2h = 0;
+    // layer callbacks waiting for their copies, run in order
+    std::deque<std::pair<cudaEvent_t, std::function<bool()>>> deferred;
+    bool run_deferred(bool all)
+    {
+        while (!deferred.empty()) {
+            auto &d = deferred.front();
+            if (!all && cudaEventQuery(d.first) == cudaErrorNotReady) return true;
+            if (!CGB_CUDA(cudaEventSynchronize(d.first))) return false;
+            cudaEventDestroy(d.first);
+            const bool ok = d.second();
+            deferred.pop_front();
+            if (!ok) {
+                set_error("host callback failed");
+                return false;
+            }
+        }
+        return true;
+    }
     bool layer(int sum, u64 *d, u64 n, cudaStream_t s, bool *kept) override
     {
         // the engine's layer buffer is reused by the next layer step: keep an
@@ -47,15 +89,26 @@ struct StoreSink : LayerSink {
         u64 *keys = store.ptr(L.h, s);
         if (!keys) return false;
         if (n && !CGB_CUDA(cudaMemcpyAsync(keys, d, n * 8, cudaMemcpyDeviceToDevice, s))) return false;
-        layers.push_back(L);
         if (fn) {
             cgb_layer_fn f = fn;
             void *u = user;
-            if (!out->enqueue({{keys, n * 8}}, [f, u, sum, n](const char *h) {
-                    return f(u, sum, (const uint64_t *)h, n) == 0;
-                }))
+            // with tables wanted too, the layer's host copy is kept for them, so
+            // the keys cross the link once; else one of the two pinned slots
+            u64 *hk = host && host->used + n * 8 + 16 <= host_cap ? (u64 *)host->take(n * 8 + 16) : nullptr;
+            if (hk) {
+                cudaEvent_t ev = copy_to_host(hk, keys, n * 8, s, out->io);
+                if (!ev) return false;
+                L.host = hk;
+                host_d2h += n * 8;
+                deferred.push_back({ev, [f, u, sum, n, hk] { return f(u, sum, hk, n) == 0; }});
+                if (!run_deferred(false)) return false;
+            } else if (!out->enqueue({{keys, n * 8}}, [f, u, sum, n](const char *h) {
+                           return f(u, sum, (const uint64_t *)h, n) == 0;
+                       })) {
                 return false;
+            }
         }
+        layers.push_back(L);
         // keep room for the next layer steps: the working set grows with the
         // layer, so the reserve scales with it
         // (the device query is not free: ask only when the store took a new chunk)
@@ -156,12 +209,19 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
     sink.reserve_bytes = e.spill_reserve;
     sink.store.chunk_bytes = e.store_chunk;
     sink.device = e.device;
+    if (w->layer_fn && w->table_fn) {
+        e.host_layers.reset();
+        sink.host = &e.host_layers;
+        sink.host_cap = e.host_layers_cap;
+    }
     GenTimes tm;
     const KernelStats k0 = kstats();
     cudaEvent_t ev[3];
     for (auto &x : ev) cudaEventCreate(&x);
     cudaEventRecord(ev[0], s);
     bool ok = e.generate(w->initial, w->n_initial, w->start, w->end_gen, sink, &tm);
+    // every layer callback has run (and every kept host copy is complete)
+    if (!sink.run_deferred(true)) ok = false;
     cudaEventRecord(ev[1], s);
 
     // ---- solve, top-down (src/solve.c:203-219) ----
@@ -234,9 +294,19 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
             const int prec = c.vbytes == 8 ? 64 : 32;
             cgb_table_fn f = w->table_fn;
             void *u = w->user;
-            ok = out.enqueue({{keys, n * 8}, {c.cur.vals, n * (u64)c.vbytes}}, [f, u, sum, n, prec](const char *h) {
-                return f(u, sum, (const uint64_t *)h, h + n * 8, n, prec) == 0;
-            });
+            static const uint64_t none = 0;
+            const u64 *hk = it != by_sum.end() ? sink.layers[it->second].host : nullptr;
+            if (hk || n == 0) {  // the keys are on the host already: copy the values only
+                const uint64_t *k = hk ? hk : &none;
+                ok = out.enqueue({{c.cur.vals, n * (u64)c.vbytes}}, [f, u, sum, n, prec, k](const char *h) {
+                    return f(u, sum, k, h, n, prec) == 0;
+                });
+            } else {
+                ok = out.enqueue({{keys, n * 8}, {c.cur.vals, n * (u64)c.vbytes}},
+                                 [f, u, sum, n, prec](const char *h) {
+                                     return f(u, sum, (const uint64_t *)h, h + n * 8, n, prec) == 0;
+                                 });
+            }
             if (!ok) break;
         }
         for (auto &c : chains) ok = ok && c.index(e, s);
@@ -275,7 +345,7 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         stats->solve_ms = solve_ms;
         stats->total_ms = gen_ms + solve_ms;
         stats->h2d_bytes = w->n_initial * 8;
-        stats->d2h_bytes = out.d2h;
+        stats->d2h_bytes = out.d2h + sink.host_d2h;
         stats->max_abs_err = max_err;
         stats->spilled_chunks = sink.store.spills;
         stats->restored_chunks = sink.store.restores;

@@ -115,6 +115,12 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         E().spill_reserve = (u64)value << 20;
+    } else if (k == "host_layers_mb") {
+        if (value < 0) {
+            set_error("cgb_set_option: host_layers_mb must be >= 0");
+            return -1;
+        }
+        E().host_layers_cap = (u64)value << 20;
     } else if (k == "store_chunk_mb") {
         if (value < 1) {
             set_error("cgb_set_option: store_chunk_mb must be >= 1");
@@ -151,6 +157,7 @@ long long cgb_get_option(const char *name)
     if (k == "spill_reserve_mb") return (long long)(E().spill_reserve >> 20);
     if (k == "max_sort_keys") return (long long)E().max_sort_keys;
     if (k == "store_chunk_mb") return (long long)(E().store_chunk >> 20);
+    if (k == "host_layers_mb") return (long long)(E().host_layers_cap >> 20);
     return -1;
 }
 

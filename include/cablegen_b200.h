@@ -44,6 +44,9 @@ int cgb_set_rules(const cgb_rules *rules);
  * (free device memory kept before resident layers spill to host memory),
  * "max_sort_keys" (larger layer steps are cut into chunks and merged),
  * "store_chunk_mb" (device allocation unit of the resident-layer store),
+ * "host_layers_mb" (pinned host memory a sweep may keep for its layers' host
+ * copies when layer and table callbacks are both given, so table keys need no
+ * second copy; default 65536),
  * "hash_load_pct" (target load factor of the hash index, 10..90, or 0, the
  * default: 25 up to 2^27 keys per table, 45 above).
  * cgb_get_option returns -1 for an unknown name. */

@@ -70,8 +70,19 @@ def test_tablebase_fp32_error(cuda, index_kind):
     assert st["max_abs_err"] == pytest.approx(err, abs=0)
 
 
-def test_tablebase_async_copies_match(cuda):
-    """Layers and tables copied out asynchronously equal the engine's own (LL, pruned, 40 layers)."""
+@pytest.mark.parametrize("host_layers_mb", [65536, 0])
+def test_tablebase_async_copies_match(cuda, host_layers_mb):
+    """Layers and tables copied out asynchronously equal the engine's own (LL, pruned, 40 layers),
+    with the layers' host copies kept for the tables (default) and without (keys copied again)."""
+    old = cuda.get_option("host_layers_mb")
+    cuda.set_option("host_layers_mb", host_layers_mb)
+    try:
+        _async_copies_case(cuda, host_layers_mb)
+    finally:
+        cuda.set_option("host_layers_mb", old)
+
+
+def _async_copies_case(cuda, host_layers_mb):
     w = configs.get("ll_pruned", end_gen=96)
     f = w.formations[0]
     cuda.set_rules(w.settings)
@@ -86,7 +97,10 @@ def test_tablebase_async_copies_match(cuda):
     vals = O.solve(lut, ost, want, f.winstates, 96, f.start)
     for s in want:
         assert np.array_equal(tables[s][1], vals[s]), s
-    assert st["d2h_bytes"] == sum(16 * len(v) for v in want.values()) + sum(8 * len(v) for v in want.values())
+    # with layers and tables both wanted, a layer's keys cross once (kept on the host for its
+    # table), so the tables carry their f64 values only; without the host copies, keys again
+    table_bytes = 8 if host_layers_mb else 16
+    assert st["d2h_bytes"] == sum(table_bytes * len(v) for v in want.values()) + sum(8 * len(v) for v in want.values())
 
 
 @pytest.mark.parametrize("index_kind", INDEX_KINDS, indirect=True)
