@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-formation batched sweep block")
     ap.add_argument("--cpu-end", type=int, default=None, help="end tile sum of the CPU sample")
+    ap.add_argument("--case", default=None, choices=["sort", "expand", "solve"],
+                    help="one small kernel case for a profiler capture instead of the benchmark")
+    ap.add_argument("--case-end", type=int, default=260, help="end tile sum of the solve case")
     return ap.parse_args()
 
 
@@ -178,8 +181,6 @@ def reference_sample(workload, end, cores, workdir=None):
     more than 127 worker threads (src/array.c:247-251).
     """
     from cablegen_b200 import configs
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    from make_golden import write_conf
     import numpy as np
     wl = configs.get(workload)
     form = wl.formations[0]
@@ -193,7 +194,7 @@ def reference_sample(workload, end, cores, workdir=None):
         np.array(form.initial, dtype="<u8").tofile(os.path.join(work, "initial"))
         np.array(form.winstates, dtype="<u8").tofile(os.path.join(work, "winstates"))
         conf = os.path.join(work, "cablegen.conf")
-        write_conf(conf, wl, form, bdir, tdir, cores, end_gen=end, end_solve=form.start)
+        configs.reference_conf(conf, wl, form, bdir, tdir, cores, end_gen=end, end_solve=form.start)
         env = dict(os.environ, XDG_CONFIG_HOME=work)
         t0 = time.perf_counter()
         subprocess.run([REF_CLI, f"-C={conf}", f"-c={cores}", "generate"], check=True, cwd=work,
@@ -441,8 +442,59 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------- kernel cases for profiler captures
+def random_ll_boards(rng, n, max_exp=9, p_empty=0.35):
+    """Seeded random LL/4422 boards (cells 10,11,14,15 fixed), tiles up to 2^max_exp."""
+    import numpy as np
+    from cablegen_b200 import configs
+    cells = configs.LL_CELLS
+    free = np.array([c for c in range(16) if c not in cells])
+    out = np.zeros(n, dtype=np.uint64)
+    for c in cells:
+        out |= np.uint64(0xF) << np.uint64(60 - 4 * c)
+    exps = rng.integers(1, max_exp + 1, size=(n, len(free))).astype(np.uint64)
+    exps[rng.random((n, len(free))) < p_empty] = 0
+    for j, c in enumerate(free):
+        out |= exps[:, j] << np.uint64(60 - 4 * int(c))
+    return out
+
+
+def run_case(args):
+    """Small stand-alone kernel cases (a few GB on the device at most), sized for
+    `ncu --set full` captures of one launch:
+      sort    ~88M LL-like canonical keys: histogram, digit passes, unique
+      expand  30M LL-like boards: moves (prune 58/5/6) and spawns
+      solve   the LL pruned workload generated and solved (FP64) up to --case-end"""
+    import numpy as np
+    import torch
+    from cablegen_b200 import configs, device
+    device.init(0)
+    w = configs.get("ll_pruned")
+    device.set_rules(w.settings)
+    rng = np.random.default_rng(5)
+    if args.case == "sort":
+        c = device.canonicalize(device.to_device(random_ll_boards(rng, 25_000_000)))
+        x = torch.cat([c, c.flip(0), c[1::2], c[::2], c[::3], c[::5]])
+        srt, p = device.sort(x)
+        u = device.unique(srt)
+        print("keys", x.numel(), "passes", p, "unique", u.numel())
+    elif args.case == "expand":
+        b = device.to_device(random_ll_boards(rng, 30_000_000))
+        o = device.expand_moves(b)
+        o2, _ = device.expand_spawns(b)
+        print("moves", o.numel(), "spawns", o2.numel())
+    else:
+        f = w.formations[0]
+        _, _, st = device.tablebase(f.initial, f.start, args.case_end, f.start, f.winstates, 64)
+        print(st)
+    print(device.kernel_stats())
+    return 0
+
+
 def main():
     args = parse()
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -4,8 +4,8 @@
 
 Every CUDA/C++ source under csrc/ is compiled to an object under _build/ and
 linked into one shared library with the CUDA runtime linked statically, so the
-library has no dependency beyond the driver.  The reference's CLI links
-against the same library.
+library has no dependency beyond the driver.  The reference's own CLI sources
+link against the same library (build_cli).
 """
 from __future__ import annotations
 

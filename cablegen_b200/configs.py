@@ -278,6 +278,48 @@ def ll_large(seed: int = SEED, end_gen: int = 1400) -> Workload:
     return w
 
 
+def reference_conf(path: str, wl: Workload, form: Formation, bdir: str, tdir: str, cores: int,
+                   end_gen: int = None, end_solve: int = None, initial: str = None, winstates: str = None) -> None:
+    """Write the reference's INI configuration for one formation of a workload.
+
+    Keys, sections and value spellings are those the reference reads
+    (src/settings.c:34-86): [Cablegen] rules, [Generate] and [Solve] paths and
+    ends.  `initial` and `winstates` default to files of those names beside
+    `path`.  Used to drive the reference CLI (the CPU baseline, the golden
+    fixtures) and the same CLI linked to this library.
+    """
+    import os
+    s = wl.settings
+    tf = lambda v: "true" if v else "false"  # noqa: E731
+    here = os.path.dirname(path)
+    initial = initial if initial is not None else os.path.join(here, "initial")
+    winstates = winstates if winstates is not None else os.path.join(here, "winstates")
+    with open(path, "w") as f:
+        f.write(f"""[Cablegen]
+free_formation = {tf(s.free_formation)}
+ignore_f = {tf(s.ignore_f)}
+cores = {cores}
+nox = {s.nox}
+use_gpu = false
+
+[Generate]
+dir = {bdir}
+initial = {initial}
+end = {end_gen if end_gen is not None else form.end_gen}
+stsl = {s.stsl}
+ltc = {s.ltc}
+smallest_large = {s.smallest_large}
+prune = {tf(s.prune)}
+
+[Solve]
+dir = {tdir}
+winstates = {winstates}
+end = {end_solve if end_solve is not None else form.end_solve}
+score = {tf(s.score)}
+delete_boards = false
+""")
+
+
 WORKLOADS = {
     "plain_2x4": plain_2x4,
     "plain_2x4_nearwall": plain_2x4_nearwall,

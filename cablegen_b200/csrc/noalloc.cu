@@ -8,15 +8,20 @@
 // digit-pass and unique kernels as cgb_sort/cgb_unique, but all of its
 // scratch (the ping-pong key buffer, digit histograms, tile counters,
 // look-back state, error word and count) lives in one file-scope
-// __device__ array of fixed size.  Every GPU that loads this library holds
-// that array (a little over 8 MiB) until the process exits.
+// __device__ array of fixed size (a little over 8 MiB).
 //
 // Limits and rules of use:
 //  * at most CGB_NOALLOC_MAX_KEYS (2^20) keys per call; larger inputs are
 //    rejected with an error, nothing is launched;
-//  * the first call on a device resolves the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make
-//    that first call before any stream capture;
+//  * set-up: the first call on a device resolves the array's device address
+//    with cudaGetSymbolAddress (with that device current) and caches it.  The
+//    CUDA runtime loads this file's device code lazily, so that first call is
+//    also when the driver places the array on the GPU -- the one moment it
+//    allocates device memory and may synchronise the device.  A call with
+//    n = 0 does only this set-up: make it once per device outside any
+//    budgeted or latency-sensitive region and before any stream capture.
+//    From then on every GPU that was set up holds the array until the
+//    process exits;
 //  * every call on a device shares the one array and leaves its contents
 //    behind; the call clears what must start at zero, but two calls whose
 //    work overlaps on the GPU (other host threads, other streams) race on
@@ -90,13 +95,13 @@ extern "C" int cgb_sort_unique_noalloc(const uint64_t *d_in, uint64_t n, uint64_
         set_error(buf);
         return -1;
     }
+    u64 *base = nullptr;
+    if (!scratch_address(&base)) return -1;  // the set-up; n = 0 stops after it
     if (n == 0) return 0;
     if (!d_in || !d_out || !n_out) {
         set_error("cgb_sort_unique_noalloc: null pointer");
         return -1;
     }
-    u64 *base = nullptr;
-    if (!scratch_address(&base)) return -1;
     cudaStream_t s = (cudaStream_t)stream;
     u64 *keys_tmp = base;                             // MAX_KEYS keys
     u32 *state = (u32 *)(base + MAX_KEYS);

@@ -25,6 +25,7 @@
 //   INDEX_HASH    open addressing with linear probing; a 16-byte slot holds
 //                 the key and the value, so a hit costs one sector
 #include "engine.h"
+#include "hashidx.cuh"
 
 namespace cgb {
 
@@ -45,21 +46,6 @@ struct DevTable {
     const ulonglong2 *slots;
     u64 cap;
 };
-
-// 32-bit hash of a board: both halves multiplied by odd constants, then
-// xor-shift / multiply rounds (constants of the murmur3 and xxhash32
-// finalisers); range-reduced by a multiply-high, so tables need not be a
-// power of two (capacity < 2^32 slots).
-__host__ __device__ __forceinline__ u32 hash32(u64 k)
-{
-    u32 x = ((u32)(k >> 32) * 0x9E3779B1u) ^ ((u32)k * 0x85EBCA77u);
-    x ^= x >> 15;
-    x *= 0xC2B2AE3Du;
-    x ^= x >> 13;
-    return x;
-}
-
-__device__ __forceinline__ u64 home_slot(u64 key, u64 cap) { return __umulhi(hash32(key), (u32)cap); }
 
 template <typename V>
 __device__ __forceinline__ V from_bits(u64 b);
@@ -597,7 +583,7 @@ int g_hash_load_pct = 0;
 u64 hash_capacity(u64 n)
 {
     const u64 pct = g_hash_load_pct ? (u64)g_hash_load_pct : (n <= (1ull << 27) ? 25 : 45);
-    return ((n * 100 + pct - 1) / pct + 63) / 64 * 64;
+    return hash_capacity_for(n, pct);
 }
 
 bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s)

@@ -82,12 +82,16 @@ int cgb_canonicalize(const uint64_t *d_in, uint64_t n, uint64_t *d_out);
  * library allocate device memory (a host whose caching allocator owns the
  * GPU under a hard budget, or latency-sensitive code that cannot absorb
  * cudaMalloc's device-wide synchronisation).  Its scratch is one fixed
- * __device__ array (a little over 8 MiB, held by every GPU that loads the
- * library until exit), so n is limited to 2^20 keys; larger n is rejected
- * with an error.  The first call on a device looks up the array's address
- * and should come before any stream capture.  Calls share the array: calls
- * that overlap on the GPU race and must be serialised.  stream may be 0.
- * Returns after the work on `stream` has finished. */
+ * __device__ array (a little over 8 MiB), so n is limited to 2^20 keys;
+ * larger n is rejected with an error.  The first call on a device is its
+ * set-up: it looks up the array's address, and because the runtime loads
+ * device code lazily, that is also when the driver places the array on the
+ * GPU (an allocation that may synchronise the device).  A call with n = 0
+ * does only the set-up: make it once per device outside any budgeted region
+ * and before any stream capture; the array then stays until the process
+ * exits.  Calls share the array: calls that overlap on the GPU race and must
+ * be serialised.  stream may be 0.  Returns after the work on `stream` has
+ * finished. */
 int cgb_sort_unique_noalloc(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t *n_out, void *stream);
 
 /* ---- solve of one layer (solve_layer, src/solve.c:289-340) ---------------

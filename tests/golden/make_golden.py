@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that holds the reference sources (default /root/reference):
+Run in a container that holds the reference sources; their path comes from the
+CABLEGEN_REFERENCE environment variable, else BASELINE.json's "reference_path":
 
-    make -C oracle all                       # builds oracle/_ref/{libcgref.so,cli}
+    make -C oracle all REF=<reference sources> # builds oracle/_ref/{libcgref.so,cli}
     python tests/golden/make_golden.py units
     python tests/golden/make_golden.py run plain_2x4 --cores 8
     python tests/golden/make_golden.py run ll_unpruned --end 120 --cores 8
@@ -43,32 +44,7 @@ REF_CLI = os.path.join(ROOT, "oracle", "_ref", "cli")
 
 def write_conf(path, wl: configs.Workload, form: configs.Formation, bdir, tdir, cores, end_gen=None,
                end_solve=None):
-    s = wl.settings
-    tf = lambda v: "true" if v else "false"
-    with open(path, "w") as f:
-        f.write(f"""[Cablegen]
-free_formation = {tf(s.free_formation)}
-ignore_f = {tf(s.ignore_f)}
-cores = {cores}
-nox = {s.nox}
-use_gpu = false
-
-[Generate]
-dir = {bdir}
-initial = {os.path.join(os.path.dirname(path), 'initial')}
-end = {end_gen if end_gen is not None else form.end_gen}
-stsl = {s.stsl}
-ltc = {s.ltc}
-smallest_large = {s.smallest_large}
-prune = {tf(s.prune)}
-
-[Solve]
-dir = {tdir}
-winstates = {os.path.join(os.path.dirname(path), 'winstates')}
-end = {end_solve if end_solve is not None else form.end_solve}
-score = {tf(s.score)}
-delete_boards = false
-""")
+    configs.reference_conf(path, wl, form, bdir, tdir, cores, end_gen=end_gen, end_solve=end_solve)
 
 
 def sha(path):

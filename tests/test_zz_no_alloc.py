@@ -2,9 +2,10 @@
 
 It exists for callers that cannot let this library allocate device memory
 (a host whose own allocator owns the GPU under a hard budget, or code that
-cannot absorb cudaMalloc's device-wide synchronisation).  The test calls it
-through the C ABI twice in a row and compares both results with the
-allocating entry points cgb_sort + cgb_unique, bit for bit (integer keys).
+cannot absorb cudaMalloc's device-wide synchronisation).  The test makes the
+set-up call (n = 0) first, then calls the entry point through the C ABI twice
+in a row and compares both results bit for bit (integer keys) with np.unique
+of the input and with the allocating entry points cgb_sort + cgb_unique.
 """
 import ctypes as C
 
@@ -51,21 +52,23 @@ def test_noalloc_matches_allocating_path(cuda):
     xs = [_inputs(seed, n) for seed, n in runs]
     xds = [cuda.to_device(x) for x in xs]
     outs = [torch.empty(n, dtype=torch.int64, device="cuda") for _, n in runs]
+    # set-up only: places the fixed scratch array on this GPU (the one allocation, by the driver)
+    cnt = C.c_uint64(5)
+    assert f(None, 0, None, C.byref(cnt), None) == 0, _lib.lib().cgb_last_error().decode()
+    assert cnt.value == 0
     results = []
-    free_before = None
     for i, (seed, n) in enumerate(runs):
         x, xd = xs[i], xds[i]
-        if i == 1:
-            torch.cuda.synchronize()
-            free_before = torch.cuda.mem_get_info()[0]
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         got = _noalloc(f, xd, n, outs[i])
-        if i == 1:
-            torch.cuda.synchronize()
-            # nothing was allocated by the call (memory can only have been freed)
-            assert torch.cuda.mem_get_info()[0] >= free_before
+        torch.cuda.synchronize()
+        # after the set-up, nothing is allocated by a call (memory can only have been freed)
+        assert torch.cuda.mem_get_info()[0] >= free_before
         assert np.array_equal(cuda.to_numpy(xd), x)   # input untouched
         results.append((xd, got))
-    for xd, got in results:
+    for (xd, got), x in zip(results, xs):
+        assert np.array_equal(cuda.to_numpy(got), np.unique(x))
         want = cuda.sort_unique(xd)                     # cgb_sort + cgb_unique
         assert got.numel() == want.numel()
         assert torch.equal(got, want)
