@@ -214,6 +214,84 @@ def default_cpu_end(workload):
     return {"ll_pruned": 160, "plain_2x4": 300, "dpdf": 340, "ll_large": 100}.get(workload, 120)
 
 
+def bench_config(workload, end=None):
+    """The workload both arms name in their JSON line (identical dicts): what one step is.
+    The reference arm times a bounded sample of it (its `sample` says which)."""
+    from cablegen_b200 import configs
+    wl = configs.get(workload) if end is None else configs.get(workload, end_gen=end)
+    form = wl.formations[0]
+    return {"workload": workload, "description": wl.description, "start": form.start, "end_gen": form.end_gen,
+            "solve": "fp64", "step": "generate start..end_gen, then solve end_gen..start",
+            "l2": "inputs larger than L2 (layers resident in HBM, tens of GB)"}
+
+
+def quiet_stdout():
+    """Context manager: the C API's log lines (stdout) go to /dev/null, so the bench prints
+    one JSON line."""
+    import contextlib
+
+    @contextlib.contextmanager
+    def cm():
+        sys.stdout.flush()
+        saved = os.dup(1)
+        null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(null, 1)
+        try:
+            yield
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+            os.close(null)
+    return cm()
+
+
+def dropin_sample(workload, end, workdir=None):
+    """The drop-in path on the reference arm's sample: the reference's public C API as this
+    library implements it (include/cablegen.h: change_config, generate, solve), called the way
+    the reference CLI calls it (frontends/cli/main.c:79-139), writing every .boards and .tables
+    file to /dev/shm.  Returns (boards processed, seconds, bytes written)."""
+    import ctypes as C
+    import numpy as np
+    from cablegen_b200 import _lib, configs
+    lib = _lib.lib()
+
+    class SArr(C.Structure):
+        _fields_ = [("valid", C.c_bool), ("bp", C.POINTER(C.c_uint64)), ("size", C.c_size_t)]
+    lib.generate.argtypes = [C.c_int, C.c_int, C.c_char_p, C.POINTER(SArr)]
+    lib.generate.restype = None
+    lib.solve.argtypes = [C.c_uint, C.c_uint, C.c_char_p, C.c_char_p, C.POINTER(SArr)]
+    lib.solve.restype = None
+    lib.change_config.argtypes = [C.c_char_p]
+    lib.change_config.restype = None
+    wl = configs.get(workload)
+    form = wl.formations[0]
+    work = workdir or tempfile.mkdtemp(prefix="cgdrop_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        bdir = os.path.join(work, "boards") + "/"
+        tdir = os.path.join(work, "tables") + "/"
+        os.makedirs(bdir, exist_ok=True)
+        os.makedirs(tdir, exist_ok=True)
+        init = np.array(form.initial, dtype=np.uint64)
+        ws = np.array(form.winstates, dtype=np.uint64)
+        init.tofile(os.path.join(work, "initial"))
+        ws.tofile(os.path.join(work, "winstates"))
+        conf = os.path.join(work, "cablegen.conf")
+        configs.reference_conf(conf, wl, form, bdir, tdir, host_cores(), end_gen=end, end_solve=form.start)
+        lib.change_config(conf.encode())
+        si = SArr(True, init.ctypes.data_as(C.POINTER(C.c_uint64)), len(init))
+        sw = SArr(True, ws.ctypes.data_as(C.POINTER(C.c_uint64)), len(ws))
+        with quiet_stdout():
+            t0 = time.perf_counter()
+            lib.generate(form.start, end, (bdir + "%d.boards").encode(), C.byref(si))
+            lib.solve(end, form.start, (bdir + "%d.boards").encode(), (tdir + "%d.tables").encode(), C.byref(sw))
+            dt = time.perf_counter() - t0
+        gen = sum(os.path.getsize(os.path.join(bdir, f)) // 8 for f in os.listdir(bdir) if f.endswith(".boards"))
+        written = sum(os.path.getsize(os.path.join(d, f)) for d in (bdir, tdir) for f in os.listdir(d))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    return 2 * gen, dt, written
+
+
 def run_reference_arm(args):
     world, rank, local = dist_env()
     if rank != 0:
@@ -237,7 +315,8 @@ def run_reference_arm(args):
             "warmup": args.warmup, "ms_per_step": 1000 * secs / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 boards)",
             "impl": "reference",
-            "config": {"workload": args.workload, "sample_end": end, "cores": min(cores, 127)},
+            "config": bench_config(args.workload, args.end),
+            "sample": {"end_gen": end, "cores": min(cores, 127), "what": desc},
             "cpu_baseline": {"value": value, "unit": "boards/s", "cores": min(cores, 127), "kind": "reference",
                              "sample": desc},
             "e2e": {"value": value, "unit": "boards/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -348,6 +427,54 @@ def run_ours(args):
                "path": "cgb_sweep_run with layer and table callbacks: layers copied once into kept pinned host "
                        "memory on the I/O stream, tables' values through pinned double buffers"}
 
+    # ---- FP32 (Kahan) against FP64 per configuration: config 2 (this workload, above),
+    # config 3 (DPDF, in full) and config 5 (LL free formation, nox 10, to the end the
+    # reference's digests pin) -- both chains side by side, max/mean |fp32 - fp64| per layer
+    precision = None
+    if not args.no_fp32 and rank == 0:
+        precision = {}
+        if fp32 is not None:
+            precision[args.workload] = {"layers": fp32["layers_checked"], "max_abs_err": fp32["max_abs_err"],
+                                        "mean_abs_err": fp32["mean_abs_err"], "end_gen": form.end_gen}
+        for name, end in (("dpdf", None), ("ll_large", 70)):
+            if name == args.workload:
+                continue
+            pw = configs.get(name) if end is None else configs.get(name, end_gen=end)
+            pf = pw.formations[0]
+            device.set_rules(pw.settings)
+            _, _, sp = device.tablebase(pf.initial, pf.start, pf.end_gen, pf.start, pf.winstates, 0)
+            pe = sp["layer_errors"]
+            pn = sum(n for n, _, _ in pe.values())
+            worst = max(pe.items(), key=lambda kv: kv[1][1]) if pe else (None, (0, 0.0, 0.0))
+            precision[name] = {"layers": len(pe), "boards": pn, "end_gen": pf.end_gen,
+                               "max_abs_err": max((mx for _, mx, _ in pe.values()), default=0.0),
+                               "mean_abs_err": (sum(n * m for n, _, m in pe.values()) / pn) if pn else 0.0,
+                               "worst_layer": worst[0], "fp64_top_layers": device.get_option("fp64_top_layers")}
+        device.set_rules(wl.settings)
+        for v in precision.values():
+            v["within_1e-6"] = v["max_abs_err"] <= 1e-6
+
+    # ---- like for like with the reference arm: the same sample (generate + solve over
+    # the reference arm's tile sums) through the drop-in C API, every file written
+    like = None
+    if not args.no_e2e and rank == 0:
+        cend = args.cpu_end or default_cpu_end(args.workload)
+        dropin_sample(args.workload, cend)  # warm-up
+        db, dsec, dbytes = 0, 0.0, 0
+        for _ in range(max(1, min(args.steps, 5))):
+            b, dt, nb = dropin_sample(args.workload, cend)
+            db += b
+            dsec += dt
+            dbytes = nb
+        device.set_rules(wl.settings)
+        like = {"value": db / dsec, "unit": "boards/s", "end_gen": cend,
+                "sample": f"generate {form.start}..{cend} then solve {cend}..{form.start} of {args.workload}, "
+                          "the reference arm's sample",
+                "path": "include/cablegen.h generate() + solve() (the calls the reference CLI makes), "
+                        ".boards and .tables files written to /dev/shm",
+                "bytes_written_per_step": dbytes, "h2d_bytes_per_step": 8 * len(form.initial),
+                "d2h_bytes_per_step": dbytes}
+
     # ---- the 64-formation batch (FP32 solve): one sweep for all formations, and
     # the same formations run one sweep each
     batch = None
@@ -423,18 +550,20 @@ def run_ours(args):
         end = args.cpu_end or default_cpu_end(args.workload)
         b, dt, desc = reference_sample(args.workload, end, cores)
         cpu = {"value": b / dt, "unit": "boards/s", "cores": min(cores, 127), "kind": "reference", "sample": desc}
+    if like is not None and cpu is not None:
+        # the same sample on both sides: the like-for-like speed-up of the drop-in path
+        like["ratio_vs_cpu_baseline"] = like["value"] / cpu["value"]
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "boards/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded SplitMix64 initial boards)",
-                "config": {"workload": args.workload, "description": wl.description, "start": form.start,
-                           "end_gen": form.end_gen, "solve": "fp64", "parallelism": f"replicas x{world}",
-                           "boards_per_step": boards // max(args.steps, 1),
-                           "l2": "inputs larger than L2 (layers resident in HBM, tens of GB)"},
+                "config": bench_config(args.workload, args.end),
+                "parallelism": f"replicas x{world}", "boards_per_step": boards // max(args.steps, 1),
                 "wall_s": wall, "gpu_launches": gpu_launches, "clocks": clock_summary, "roofline": roofline,
-                "fp32": fp32, "e2e": e2e, "batch": batch, "cpu_baseline": cpu}
+                "fp32": fp32, "precision": precision, "e2e": e2e, "like_for_like": like, "batch": batch,
+                "cpu_baseline": cpu}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

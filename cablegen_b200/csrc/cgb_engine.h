@@ -131,6 +131,7 @@ struct Engine {
     u64 spill_reserve = 24ull << 30;  // free device memory kept before spilling resident layers
     u64 max_sort_keys = 1ull << 28;   // larger layer steps are cut into chunks and merged
     u64 store_chunk = 4ull << 30;     // device allocation unit of the resident-layer store
+    int fp64_top_layers = 4;          // FP32 sweeps: the highest layers solved in FP64
     FormationFilter filter;           // batched sweeps: formations that still generate
 
     static Engine &get();

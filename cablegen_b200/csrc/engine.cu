@@ -18,6 +18,7 @@
 #include "cgb_engine.h"
 #include <algorithm>
 #include <mutex>
+#include <unordered_map>
 
 namespace cgb {
 
@@ -103,10 +104,28 @@ void KClock::flush()
 }
 
 // ---- memory -----------------------------------------------------------------
+// Every engine allocation goes through dev_alloc/dev_free, which count the
+// bytes held, so that a cap (option device_mem_cap_mb: a host whose allocator
+// gives this library a fixed budget) turns into a clean allocation failure.
+u64 g_dev_mem_cap = 0;
+static std::mutex g_mem_mu;
+static std::unordered_map<void *, u64> g_mem_blocks;
+static u64 g_mem_held = 0;
+
 bool dev_alloc(void **p, u64 bytes, cudaStream_t s)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 256;
+    {
+        std::lock_guard<std::mutex> g(g_mem_mu);
+        if (g_dev_mem_cap && g_mem_held + bytes > g_dev_mem_cap) {
+            char buf[200];
+            snprintf(buf, sizeof buf, "device allocation of %.3f GB failed: over the cap of %.3f GB (%.3f GB held)",
+                     bytes / 1e9, g_dev_mem_cap / 1e9, g_mem_held / 1e9);
+            set_error(buf);
+            return false;
+        }
+    }
     cudaError_t e = cudaMallocAsync(p, bytes, s);
     if (e == cudaErrorMemoryAllocation) {
         // freed blocks of other sizes may still sit in the pool: return them
@@ -124,13 +143,26 @@ bool dev_alloc(void **p, u64 bytes, cudaStream_t s)
         snprintf(buf, sizeof buf, "device allocation of %.3f GB failed: %s", bytes / 1e9, cudaGetErrorString(e));
         set_error(buf);
         cudaGetLastError();
+        *p = nullptr;
         return false;
     }
+    std::lock_guard<std::mutex> g(g_mem_mu);
+    g_mem_blocks[*p] = bytes;
+    g_mem_held += bytes;
     return true;
 }
 void dev_free(void *p, cudaStream_t s)
 {
-    if (p) cudaFreeAsync(p, s);
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> g(g_mem_mu);
+        auto it = g_mem_blocks.find(p);
+        if (it != g_mem_blocks.end()) {
+            g_mem_held -= it->second;
+            g_mem_blocks.erase(it);
+        }
+    }
+    cudaFreeAsync(p, s);
 }
 
 // free device memory plus what the stream-ordered pool holds cached but unused

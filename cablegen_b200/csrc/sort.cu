@@ -45,10 +45,18 @@ constexpr int MRG_TILE = MRG_THREADS * MRG_KPT;
 #ifndef LB_BATCH
 #define LB_BATCH 4
 #endif
+// Polls a look-back wait makes before it gives up (SPIN_LIMIT unless a test
+// lowers it), and a test switch that keeps tile 0 of a digit pass from
+// publishing its counts: tile 1 then waits on a flag that nothing sets, runs
+// out of polls and reports ERR_LOOKBACK_TIMEOUT (the bounded-wait path).
+__device__ u32 g_spin_limit = SPIN_LIMIT;
+__device__ u32 g_hold_first_tile = 0;
+
 __device__ __forceinline__ u32 lookback_sum(const u32 *words, u64 stride, int j, u32 *err)
 {
     u32 excl = 0;
     u32 spins = 0;
+    const u32 limit = g_spin_limit;
     while (j >= 0) {
         u32 v[LB_BATCH];
 #pragma unroll
@@ -68,7 +76,7 @@ __device__ __forceinline__ u32 lookback_sum(const u32 *words, u64 stride, int j,
         }
         if (done) break;
         if (stalled) {
-            if (++spins > SPIN_LIMIT) {
+            if (++spins > limit) {
                 atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 break;
             }
@@ -186,7 +194,7 @@ __global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__res
     u32 *lb = lookback + (u64)tile * RADIX + d;
     u32 excl = 0;
     if (tile == 0) {
-        st_relaxed(lb, LB_PRE | cnt);
+        if (!g_hold_first_tile) st_relaxed(lb, LB_PRE | cnt);
     } else {
         st_relaxed(lb, LB_AGG | cnt);
         excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
@@ -304,7 +312,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 5)
         cnt += c;
     }
     u32 *lb = lookback + (u64)tile * RADIX + d;
-    st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
+    if (tile != 0 || !g_hold_first_tile) st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
     u32 total;
     const u32 lstart = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
     bin_local[d] = lstart;
@@ -453,7 +461,7 @@ __global__ void __launch_bounds__(SORT_THREADS, PIPE_MINB)
             cnt += c;
         }
         u32 *lb = lookback + (u64)tile * RADIX + d;
-        st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
+        if (tile != 0 || !g_hold_first_tile) st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
         const u32 lstart = block_exclusive_scan<u32>(cnt, S.scan, &total);  // (C) inside
         S.bin_local[d] = lstart;
         // keys to registers, then (E) the local scatter may overwrite buf[cur]
@@ -507,6 +515,15 @@ static int pipe_grid(int device)
 }
 
 int g_sort_variant = 1;  // 0: match-based ranking, 1: ballot-based ranking, 2: pipelined persistent
+
+// test switches of the look-back waits (see g_spin_limit); 0 restores the default limit
+bool set_lookback_test(u32 spin_limit, int hold_first_tile)
+{
+    const u32 lim = spin_limit ? spin_limit : SPIN_LIMIT;
+    const u32 hold = hold_first_tile ? 1u : 0u;
+    return CGB_CUDA(cudaMemcpyToSymbol(g_spin_limit, &lim, sizeof lim)) &&
+           CGB_CUDA(cudaMemcpyToSymbol(g_hold_first_tile, &hold, sizeof hold));
+}
 
 // ---------------------------------------------------------------------------
 // padded shared-memory index for blocked reads of 16 consecutive u64
@@ -609,7 +626,7 @@ __device__ __forceinline__ u64 tile_lookback64(u64 *lookback, u32 tile, u64 coun
         const u64 v = ld_relaxed64(lookback + j);
         const u64 flag = v & ~LB64_MASK;
         if (flag == 0) {
-            if (++spins > SPIN_LIMIT) {
+            if (++spins > g_spin_limit) {
                 atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 break;
             }
@@ -708,14 +725,17 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
         have_prev = true;
     }
     u32 flags = 0;
+    bool descent = false;  // sorted inputs merge into a non-decreasing sequence
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++) {
         if (t0 + i < t1) {
             if (!have_prev || v[i] != prev) flags |= 1u << i;
+            descent |= have_prev && v[i] < prev;
             prev = v[i];
             have_prev = true;
         }
     }
+    if (descent) atomicOr(err, ERR_UNSORTED);
     const u32 cnt = __popc(flags);
     u32 tile_total;
     const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &tile_total);

@@ -23,6 +23,8 @@ using namespace cgb;
 
 namespace {
 
+bool narrow_values(const double *a, float *b, u64 n, cudaStream_t s);
+
 struct Layer {
     int sum;
     LayerStore::Handle h;
@@ -123,11 +125,16 @@ struct StoreSink : LayerSink {
     }
 };
 
-// one precision's solve state: the current layer and the two above it
+// one precision's solve state: the current layer and the two above it.  An
+// FP32 chain solves its `fp64_above` window -- the highest layers, solved
+// first, whose values come straight from the winstates -- in FP64 and narrows
+// those tables to FP32 when the first FP32 layer below needs them.
 struct Chain {
     int vbytes = 8;
+    int fp64_above = 1 << 30;  // FP32 chain: layers with sum > this are solved in FP64
     struct Solved {
         int sum = 0;
+        int vb = 8;  // bytes per value of this layer's table
         const u64 *keys = nullptr;
         void *vals = nullptr;
         u64 n = 0;
@@ -136,10 +143,29 @@ struct Chain {
     };
     Solved t2, t4, cur;
 
+    int layer_vbytes(int sum) const { return vbytes == 4 && sum > fp64_above ? 8 : vbytes; }
+
+    // an FP64 table of the window turned into the FP32 table the chain below reads
+    bool narrow(Engine &e, Solved &x, cudaStream_t s)
+    {
+        if (x.vb == 4 || !x.vals) return true;
+        void *f = nullptr;
+        if (!dev_alloc(&f, x.n * 4 + 8, s)) return false;
+        if (x.n && !narrow_values((const double *)x.vals, (float *)f, x.n, s)) return false;
+        dev_free(x.vals, s);
+        x.vals = f;
+        x.vb = 4;
+        x.ix.keys = x.keys;
+        x.ix.vals = x.vals;
+        x.ix.n = x.n;
+        return build_index(x.ix, e.index_kind, 4, x.store, e.bucket_bits, e.ctr, s);
+    }
     bool solve(Engine &e, const SolveRules &r, cudaStream_t s)
     {
-        if (!dev_alloc(&cur.vals, cur.n * vbytes + 8, s)) return false;
-        if (vbytes == 4) return solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
+        cur.vb = layer_vbytes(cur.sum);
+        if (cur.vb == 4 && !(narrow(e, t2, s) && narrow(e, t4, s))) return false;
+        if (!dev_alloc(&cur.vals, cur.n * cur.vb + 8, s)) return false;
+        if (cur.vb == 4) return solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
         return solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
     }
     bool index(Engine &e, cudaStream_t s)
@@ -147,7 +173,7 @@ struct Chain {
         cur.ix.keys = cur.keys;
         cur.ix.vals = cur.vals;
         cur.ix.n = cur.n;
-        return build_index(cur.ix, e.index_kind, vbytes, cur.store, e.bucket_bits, e.ctr, s);
+        return build_index(cur.ix, e.index_kind, cur.vb, cur.store, e.bucket_bits, e.ctr, s);
     }
     void rotate(cudaStream_t s)
     {
@@ -166,6 +192,20 @@ struct Chain {
         }
     }
 };
+
+__global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, u64 n)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+bool narrow_values(const double *a, float *b, u64 n, cudaStream_t s)
+{
+    const int grid = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
+    narrow_kernel<<<grid, 256, 0, s>>>(a, b, n);
+    kstats().launches++;
+    return CGB_CUDA(cudaGetLastError());
+}
 
 // max and sum of |a - b| over a layer (a: fp64, b: fp32)
 __global__ void abs_diff_kernel(const double *__restrict__ a, const float *__restrict__ b, u64 n, u64 *max_bits,
@@ -238,6 +278,7 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         chains.resize(1);
         chains[0].vbytes = w->precision == 32 ? 4 : 8;
     }
+    for (auto &c : chains) c.fp64_above = w->end_gen - 2 * e.fp64_top_layers;
     u64 *d_err = nullptr;  // [max bits, sum]
     u64 solved = 0;
     double max_err = 0;
@@ -266,7 +307,14 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         }
         if (!ok) break;
         solved += n;
-        if (w->precision == 0 && n) {
+        if (w->precision == 0 && n && chains[1].cur.vb == 8) {
+            // the FP32 chain's FP64 window: the same operations on the same tables as chain 0
+            if (w->error_fn && w->error_fn(w->user, sum, n, 0.0, 0.0) != 0) {
+                set_error("error callback failed");
+                ok = false;
+                break;
+            }
+        } else if (w->precision == 0 && n) {
             ok = CGB_CUDA(cudaMemsetAsync(d_err, 0, 16, s));
             const int grid = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
             kstats().launches++;
@@ -291,18 +339,18 @@ extern "C" int cgb_sweep_run(const cgb_sweep *w, cgb_stats *stats)
         if (w->table_fn) {
             enqueued = true;
             Chain &c = chains[0];
-            const int prec = c.vbytes == 8 ? 64 : 32;
+            const int prec = c.cur.vb == 8 ? 64 : 32;
             cgb_table_fn f = w->table_fn;
             void *u = w->user;
             static const uint64_t none = 0;
             const u64 *hk = it != by_sum.end() ? sink.layers[it->second].host : nullptr;
             if (hk || n == 0) {  // the keys are on the host already: copy the values only
                 const uint64_t *k = hk ? hk : &none;
-                ok = out.enqueue({{c.cur.vals, n * (u64)c.vbytes}}, [f, u, sum, n, prec, k](const char *h) {
+                ok = out.enqueue({{c.cur.vals, n * (u64)c.cur.vb}}, [f, u, sum, n, prec, k](const char *h) {
                     return f(u, sum, k, h, n, prec) == 0;
                 });
             } else {
-                ok = out.enqueue({{keys, n * 8}, {c.cur.vals, n * (u64)c.vbytes}},
+                ok = out.enqueue({{keys, n * 8}, {c.cur.vals, n * (u64)c.cur.vb}},
                                  [f, u, sum, n, prec](const char *h) {
                                      return f(u, sum, (const uint64_t *)h, h + n * 8, n, prec) == 0;
                                  });

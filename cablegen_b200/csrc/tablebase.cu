@@ -34,6 +34,10 @@ SolveRules make_solve_rules(const cgb_rules &r, const u64 *d_ws, int nws)
 }  // namespace cgb
 
 namespace cgb {
+bool set_lookback_test(u32 spin_limit, int hold_first_tile);
+extern u64 g_dev_mem_cap;
+static u32 g_test_spin = 0;
+static int g_test_hold = 0;
 extern int g_solve_variant;
 extern int g_sort_variant;
 extern int g_hash_load_pct;
@@ -133,6 +137,31 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         E().max_sort_keys = (u64)value;
+    } else if (k == "lookback_spin_limit" || k == "lookback_hold_first_tile") {
+        // failure-path tests: a lower poll limit for look-back waits (0 = default), and a
+        // digit pass whose tile 0 never publishes, so tile 1's wait must run out
+        if (value < 0 || value > 0xFFFFFFFFll) {
+            set_error("cgb_set_option: " + k + " must be in 0..2^32-1");
+            return -1;
+        }
+        if (!E().ready && !E().init(0)) return -1;
+        if (k == "lookback_spin_limit") g_test_spin = (u32)value;
+        else g_test_hold = value ? 1 : 0;
+        if (!set_lookback_test(g_test_spin, g_test_hold)) return -1;
+    } else if (k == "device_mem_cap_mb") {
+        // a capped device allocator: allocations through the engine fail once the
+        // bytes it holds would exceed the cap (0 = no cap)
+        if (value < 0) {
+            set_error("cgb_set_option: device_mem_cap_mb must be >= 0");
+            return -1;
+        }
+        g_dev_mem_cap = (u64)value << 20;
+    } else if (k == "fp64_top_layers") {
+        if (value < 0 || value > 100000) {
+            set_error("cgb_set_option: fp64_top_layers must be in 0..100000");
+            return -1;
+        }
+        E().fp64_top_layers = (int)value;
     } else if (k == "bucket_bits") {
         if (value < 0 || value > 30) {
             set_error("cgb_set_option: bucket_bits must be in 0..30");
@@ -158,6 +187,10 @@ long long cgb_get_option(const char *name)
     if (k == "max_sort_keys") return (long long)E().max_sort_keys;
     if (k == "store_chunk_mb") return (long long)(E().store_chunk >> 20);
     if (k == "host_layers_mb") return (long long)(E().host_layers_cap >> 20);
+    if (k == "fp64_top_layers") return E().fp64_top_layers;
+    if (k == "lookback_spin_limit") return g_test_spin;
+    if (k == "lookback_hold_first_tile") return g_test_hold;
+    if (k == "device_mem_cap_mb") return (long long)(g_dev_mem_cap >> 20);
     return -1;
 }
 

@@ -48,7 +48,10 @@ int cgb_set_rules(const cgb_rules *rules);
  * copies when layer and table callbacks are both given, so table keys need no
  * second copy; default 65536),
  * "hash_load_pct" (target load factor of the hash index, 10..90, or 0, the
- * default: 25 up to 2^27 keys per table, 45 above).
+ * default: 25 up to 2^27 keys per table, 45 above),
+ * "fp64_top_layers" (FP32 sweeps of cgb_sweep_run: the highest layers, solved
+ * first, whose values come straight from the winstates, are solved in FP64 and
+ * narrowed to FP32 for the layers below; default 4, 0 = none).
  * cgb_get_option returns -1 for an unknown name. */
 int cgb_set_option(const char *name, long long value);
 long long cgb_get_option(const char *name);

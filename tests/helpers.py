@@ -31,6 +31,48 @@ def sha_table(keys, vals) -> str:
     return h.hexdigest()
 
 
+def sweep_digests(cuda, form, precision=64):
+    """Generate and solve one formation (tile sums start..end_gen, solve down to start) and
+    return ({sum: SHA-256 of the layer file}, {sum: SHA-256 of the table file}, stats): the
+    digests the reference's .boards and .tables files would have.  Layers and tables reach
+    the host through the sweep's callbacks and are hashed on a thread pool."""
+    import ctypes as C
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    workers = max(2, min(16, (os.cpu_count() or 4) - 1))
+    pool = ThreadPoolExecutor(max_workers=workers)
+    gate = threading.Semaphore(2 * workers)   # bound the bytes waiting to be hashed
+    got_layers, got_tables, futures = {}, {}, []
+
+    def digest(store, key, parts):
+        try:
+            h = hashlib.sha256()
+            for p in parts:
+                h.update(p)
+            store[key] = h.hexdigest()
+        finally:
+            gate.release()
+
+    def on_layer(s, ptr, n):
+        gate.acquire()
+        data = C.string_at(ptr, 8 * n) if n else b""
+        futures.append(pool.submit(digest, got_layers, s, [data]))
+
+    def on_table(s, kptr, vptr, n, prec):
+        assert prec == 64
+        gate.acquire()
+        keys = C.string_at(kptr, 8 * n) if n else b""
+        vals = C.string_at(vptr, 8 * n) if n else b""
+        futures.append(pool.submit(digest, got_tables, s, [keys, vals]))
+
+    _, _, st = cuda.tablebase(form.initial, form.start, form.end_gen, form.start, form.winstates,
+                              precision=precision, layer_fn=on_layer, table_fn=on_table)
+    for fu in futures:
+        fu.result()
+    pool.shutdown()
+    return got_layers, got_tables, st
+
+
 def realistic_boards(rng, n, formation_cells=(10, 11, 14, 15), max_exp=10, p_empty=0.35):
     """Random boards of a formation: 0xf fixed cells, empties and tiles."""
     cells = np.array([c for c in range(16) if c not in formation_cells])

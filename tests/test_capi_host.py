@@ -166,6 +166,31 @@ def test_board_and_table_files_round_trip(lib, tmp_path):
     assert not missing.valid
 
 
+def test_truncated_boards_file_warns_and_counts_whole_boards(tmp_path):
+    """A .boards file whose size is not a multiple of 8 is read with a warning and its whole
+    boards only (src/generate.c:616-648)."""
+    import subprocess
+    import sys
+    data = (np.arange(1, 101, dtype=np.uint64) * 0x0123456789ABCDEF)
+    path = tmp_path / "t.boards"
+    path.write_bytes(data.tobytes() + b"\x01\x02\x03")
+    code = (
+        "import ctypes as C, sys\n"
+        "class SArr(C.Structure):\n"
+        "    _fields_ = [('valid', C.c_bool), ('bp', C.POINTER(C.c_uint64)), ('size', C.c_size_t)]\n"
+        f"L = C.CDLL({LIB!r})\n"
+        "L.read_boards.argtypes = [C.c_char_p]\n"
+        "L.read_boards.restype = SArr\n"
+        f"r = L.read_boards({str(path)!r}.encode())\n"
+        "sys.stdout.flush()\n"
+        "print('RESULT', int(r.valid), r.size, r.bp[0], r.bp[r.size - 1])\n")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True,
+                         env=dict(os.environ, XDG_CONFIG_HOME=str(tmp_path))).stdout
+    assert "[WARN] sz %8 != 0, this is probably not a real table!" in out
+    res = [line for line in out.splitlines() if line.startswith("RESULT")][0].split()
+    assert res[1:] == ["1", "100", str(int(data[0])), str(int(data[-1]))]
+
+
 def test_settings_from_ini(lib, tmp_path):
     conf = tmp_path / "c.conf"
     conf.write_text("""; comment

@@ -70,6 +70,31 @@ def test_tablebase_fp32_error(cuda, index_kind):
     assert st["max_abs_err"] == pytest.approx(err, abs=0)
 
 
+@pytest.mark.parametrize("top", [0, 6])
+def test_tablebase_fp32_fp64_window(cuda, top):
+    """An FP32 sweep solves its `fp64_top_layers` highest layers in FP64 (bit-equal to the FP64
+    sweep's tables there) and narrows them for the FP32 layers below, which stay within 1e-6."""
+    w = configs.get("plain_2x4_nearwall")
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    old = cuda.get_option("fp64_top_layers")
+    try:
+        cuda.set_option("fp64_top_layers", top)
+        _, t64, _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=64, keep_tables=True)
+        _, t32, _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=32, keep_tables=True)
+    finally:
+        cuda.set_option("fp64_top_layers", old)
+    window = [s for s in t32 if s > f.end_gen - 2 * top]
+    assert len(window) == top
+    for s in t32:
+        if s in window:
+            assert t32[s][1].dtype == np.float64 and np.array_equal(t32[s][1], t64[s][1]), s
+        else:
+            assert t32[s][1].dtype == np.float32, s
+            if len(t32[s][1]):
+                assert np.abs(t64[s][1] - t32[s][1].astype(np.float64)).max() <= 1e-6, s
+
+
 @pytest.mark.parametrize("host_layers_mb", [65536, 0])
 def test_tablebase_async_copies_match(cuda, host_layers_mb):
     """Layers and tables copied out asynchronously equal the engine's own (LL, pruned, 40 layers),
