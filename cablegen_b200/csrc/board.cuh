@@ -243,29 +243,77 @@ __host__ __device__ __forceinline__ bool matches(u64 b, u64 w)
 }
 
 // ---- the row table in shared memory -------------------------------------
-// move[row]: the row after a left move; ok bit set = the move keeps every 0xf
-// cell in place (the reference's _locked_lut, src/board.c:29-38,117).
+// move[row]: the row after a left move.  A row whose move would take a 0xf
+// cell out of place (the reference's _locked_lut, src/board.c:29-38,117) holds
+// ROW_LOCKED instead: a left move never yields 0x0001 (empty cells, then a
+// tile that did not slide), so the value is free to mark "illegal" and the
+// table needs no second bitset (build_row_table checks this for every row).
+constexpr unsigned short ROW_LOCKED = 0x0001;
+
 struct RowTable {
-    const unsigned short *move;  // 65536 entries
-    const u32 *ok;               // 2048 words, one bit per row
+    const unsigned short *move;  // 65536 entries, ROW_LOCKED for locked rows
 };
 
 // left move of the four rows of y; returns 0 when any row is locked, else
 // sets *out and returns 1 + (changed ? 1 : 0)
 __device__ __forceinline__ int move_left(const RowTable &t, u64 y, u64 *out)
 {
-    u64 r = 0;
-    bool ok = true, changed = false;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const u32 row = (u32)(y >> (16 * i)) & 0xFFFFu;
-        const u32 m = t.move[row];
-        ok &= (t.ok[row >> 5] >> (row & 31)) & 1u;
-        changed |= (m != row);
-        r |= (u64)m << (16 * i);
-    }
+    const u32 hi = (u32)(y >> 32), lo = (u32)y;
+    const u32 m0 = t.move[hi >> 16], m1 = t.move[hi & 0xFFFFu];
+    const u32 m2 = t.move[lo >> 16], m3 = t.move[lo & 0xFFFFu];
+    const bool locked = (m0 == ROW_LOCKED) | (m1 == ROW_LOCKED) | (m2 == ROW_LOCKED) | (m3 == ROW_LOCKED);
+    const u64 r = make64(__byte_perm(m1, m0, 0x5410), __byte_perm(m3, m2, 0x5410));
     *out = r;
-    return ok ? 1 + (int)changed : 0;
+    return locked ? 0 : 1 + (int)(r != y);
+}
+
+// ---- canonical form from a subset of the images ---------------------------
+// A 0xf nibble is larger than any tile, so among the 8 images of a board the
+// maximum is one whose run of leading 0xf cells (from cell 0) is longest.
+// With fixed formation cells (free_formation off) a legal move keeps every
+// 0xf cell in place, so the 0xf-mask of a move result in view k of a board is
+// the view of the board's mask, and the images that can be the maximum are
+// known before the move: canon_cand() takes the maximum over those only.
+// CanonPlan holds them for boards whose fixed_pattern() equals `mask`; a
+// board with any other mask uses all eight (cand 0xff).
+struct CanonPlan {
+    u32 mask = 0xFFFFFFFFu;      // fixed_pattern() the plan is for (never equal: no plan)
+    unsigned char view[4] = {0xFF, 0xFF, 0xFF, 0xFF};  // images for a move result in view k
+};
+
+// cand: bit i = image i of images() (id, V, H, VH, T, VT, HT, VHT)
+__host__ __device__ __forceinline__ u64 canon_cand(u64 m, u32 cand)
+{
+    if (cand == 0xFFu) return canonical(m);
+    const Half h = halves(m);
+    u64 best = 0;
+    if (cand & 0x0Fu) {
+        if (cand & 0x01u) best = umax64(best, m);
+        if (cand & 0x02u) best = umax64(best, whole(flip_v(h)));
+        if (cand & 0x0Cu) {
+            const Half hh = flip_h(h);
+            if (cand & 0x04u) best = umax64(best, whole(hh));
+            if (cand & 0x08u) best = umax64(best, whole(flip_v(hh)));
+        }
+    }
+    if (cand & 0xF0u) {
+        const Half t = transpose(h);
+        if (cand & 0x10u) best = umax64(best, whole(t));
+        if (cand & 0x20u) best = umax64(best, whole(flip_v(t)));
+        if (cand & 0xC0u) {
+            const Half th = flip_h(t);
+            if (cand & 0x40u) best = umax64(best, whole(th));
+            if (cand & 0x80u) best = umax64(best, whole(flip_v(th)));
+        }
+    }
+    return best;
+}
+
+__host__ __device__ __forceinline__ int leading_f(u64 b)
+{
+    int n = 0;
+    while (n < 16 && ((b >> (60 - 4 * n)) & 0xF) == 0xF) n++;
+    return n;
 }
 
 // the four move views of b: {b, H b, T b, H T b} for left, right, up, down
@@ -282,6 +330,33 @@ __host__ __device__ __forceinline__ void views(u64 b, u64 v[4])
 __host__ __device__ __forceinline__ int view_cell(int k, int c)
 {
     return image_cell(k == 0 ? 0 : k == 1 ? 2 : k == 2 ? 4 : 6, c);
+}
+
+// the plan for boards whose 0xf cells are those of `b` (host side, once per
+// sweep): for each view k, the images of view_k(mask) with the longest run of
+// leading 0xf cells.  free_formation lets 0xf cells move: no plan.
+inline CanonPlan make_canon_plan(u64 b, bool free_formation)
+{
+    CanonPlan p;
+    if (free_formation) return p;
+    u64 x = 0;  // the 0xf cells of b, every other cell empty
+    for (int c = 0; c < 16; c++)
+        if (((b >> (60 - 4 * c)) & 0xF) == 0xF) x |= 0xFull << (60 - 4 * c);
+    if (x == 0) return p;
+    u64 v[4];
+    views(x, v);
+    for (int k = 0; k < 4; k++) {
+        u64 im[8];
+        images(v[k], im);
+        int best = -1;
+        for (int i = 0; i < 8; i++) best = leading_f(im[i]) > best ? leading_f(im[i]) : best;
+        unsigned char cand = 0;
+        for (int i = 0; i < 8; i++)
+            if (leading_f(im[i]) == best) cand |= (unsigned char)(1u << i);
+        p.view[k] = best > 0 ? cand : 0xFF;
+    }
+    p.mask = fixed_pattern(b);
+    return p;
 }
 
 }  // namespace cgb

@@ -133,6 +133,7 @@ struct Engine {
     u64 store_chunk = 4ull << 30;     // device allocation unit of the resident-layer store
     int fp64_top_layers = 4;          // FP32 sweeps: the highest layers solved in FP64
     FormationFilter filter;           // batched sweeps: formations that still generate
+    CanonPlan plan;                   // images that can be canonical for the sweep's 0xf mask
 
     static Engine &get();
     bool init(int dev);

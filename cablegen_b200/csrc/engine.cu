@@ -396,7 +396,7 @@ bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
     for (u64 off = 0; off < n || (n == 0 && off == 0); off += m0) {
         const u64 m = std::min(m0, n - off);
         u64 nr = 0;
-        if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s, filter)) return false;
+        if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s, filter, plan)) return false;
         u64 nu = 0;
         DevBuf<u64> *u = nullptr;
         if (!sort_unique_step(g.a, g.b, nr, &nu, &u, tm)) return false;
@@ -444,7 +444,7 @@ bool Engine::spawn_layer(GenTimes *tm)
             }
         }
         u64 ns = 0;
-        if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s)) return false;
+        if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s, plan)) return false;
         // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort
         // c[1] with the buffer the first sort left free
         DevBuf<u64> *u2 = nullptr, *u4 = nullptr;
@@ -476,6 +476,9 @@ bool Engine::generate(const u64 *h_initial, u64 n_init, int start, int end, Laye
     if (n_carry && !CGB_CUDA(cudaMemcpyAsync(g.u4.p, h_carry, n_carry * 8, cudaMemcpyHostToDevice, s))) return false;
     g.S.n = n_init;
     g.u4.n = n_carry;
+    // canonical layer boards share the 0xf mask of the canonical first board (fixed
+    // formation cells); the kernels check every board against it
+    plan = (n_init && !filter.fid) ? make_canon_plan(canonical(h_initial[0]), rules.free_formation != 0) : CanonPlan{};
     bool ok = true;
     for (int layer = start; layer <= end && ok; layer += 2) {
         ok = move_layer(g.S.p, g.S.n, tm);

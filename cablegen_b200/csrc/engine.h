@@ -39,8 +39,7 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
 
 // ---- row table and expansion (expand.cu) ---------------------------------
 struct DeviceRowTable {
-    unsigned short *move = nullptr;  // 65536 rows, left move
-    u32 *ok = nullptr;               // 2048 words: bit set = the move keeps 0xf cells
+    unsigned short *move = nullptr;  // 65536 rows, left move; ROW_LOCKED where a 0xf cell would move
     int free_formation = -1, ignore_f = -1;
 };
 
@@ -59,12 +58,13 @@ struct Counters {
 bool partition_by_formation(const u64 *in, u64 n, u64 *out, const unsigned char *fid, u32 counts[256],
                             SortWorkspace &ws, cudaStream_t s);
 bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
-                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff = FormationFilter{});
+                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff = FormationFilter{},
+                  const CanonPlan &plan = CanonPlan{});
 // number of empty cells over all boards (exact size of the spawn streams)
 bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s);
 // canonical 2-spawn and 4-spawn of every empty cell of every board
 bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c,
-                   cudaStream_t s);
+                   cudaStream_t s, const CanonPlan &plan = CanonPlan{});
 
 // ---- solve (solve.cu) ------------------------------------------------------
 struct SolveRules {
@@ -120,10 +120,13 @@ bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *e
 bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
                  cudaStream_t s);
 
+// plan: images that can be canonical for the layer's 0xf mask (CanonPlan{}: all eight)
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
-                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s);
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s,
+                     const CanonPlan &plan = CanonPlan{});
 bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, const LayerIndex &t4,
-                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s);
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s,
+                     const CanonPlan &plan = CanonPlan{});
 
 // ---- device memory --------------------------------------------------------
 template <typename T>

@@ -3,11 +3,13 @@
 // expand_moves restates the move workers of the reference
 // (src/generate.c:133-175, OpenCL move_kernel src/cl/generate.cl:249-282):
 // optional prune of the input, the four moves, prune of each moved board,
-// canonicalisation.  The left-move row table (128 KiB of u16 + an 8 KiB
-// "keeps 0xf in place" bitset) is staged into shared memory once per CTA of a
+// canonicalisation.  The left-move row table (128 KiB of u16, locked rows
+// marked ROW_LOCKED) is staged into shared memory once per CTA of a
 // persistent grid; right/up/down reuse it through the board views of
-// board.cuh.  Results are appended with one atomic per CTA iteration after a
-// block scan, so the output is compact (no 4N slot array + separate scan).
+// board.cuh.  Canonical forms take the maximum over the images a CanonPlan
+// names for the board's 0xf mask (all eight without a plan).  Results are
+// appended with one atomic per CTA iteration after a block scan, so the
+// output is compact (no 4N slot array + separate scan).
 //
 // expand_spawns restates src/generate.c:177-199: every empty cell receives a
 // 2 (nibble 1) and a 4 (nibble 2); both boards are canonicalised.  The exact
@@ -18,7 +20,7 @@
 namespace cgb {
 
 constexpr int EXP_THREADS = 1024;
-constexpr int TABLE_BYTES = 65536 * 2 + 2048 * 4;
+constexpr int TABLE_BYTES = 65536 * 2;  // the left-move rows, ROW_LOCKED marking locked ones
 
 void build_row_table(int free_formation, int ignore_f, unsigned short *move, u32 *ok)
 {
@@ -68,21 +70,28 @@ bool upload_row_table(DeviceRowTable &t, int free_formation, int ignore_f, cudaS
     std::vector<unsigned short> mv(65536);
     std::vector<u32> ok(2048);
     build_row_table(free_formation, ignore_f, mv.data(), ok.data());
+    // the device table marks locked rows with ROW_LOCKED; no legal move yields it
+    for (u32 row = 0; row < 65536; row++) {
+        const bool legal = (ok[row >> 5] >> (row & 31)) & 1u;
+        if (legal && mv[row] == ROW_LOCKED) {
+            set_error("upload_row_table: a legal row move yields the locked-row marker");
+            return false;
+        }
+        if (!legal) mv[row] = ROW_LOCKED;
+    }
     if (!t.move) {
         void *p = nullptr;
         if (!CGB_CUDA(cudaMalloc(&p, TABLE_BYTES))) return false;
         t.move = (unsigned short *)p;
-        t.ok = (u32 *)((char *)p + 65536 * 2);
     }
     if (!CGB_CUDA(cudaMemcpyAsync(t.move, mv.data(), 65536 * 2, cudaMemcpyHostToDevice, s))) return false;
-    if (!CGB_CUDA(cudaMemcpyAsync(t.ok, ok.data(), 2048 * 4, cudaMemcpyHostToDevice, s))) return false;
     if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     t.free_formation = free_formation;
     t.ignore_f = ignore_f;
     return true;
 }
 
-__device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned short *g_move, const u32 *g_ok)
+__device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned short *g_move)
 {
     const uint4 *src = (const uint4 *)g_move;
     uint4 *dst = (uint4 *)smem;
@@ -93,14 +102,14 @@ __device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned 
 __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
-                                                                      const u32 *g_ok, PruneParams pp, u32 *err,
-                                                                      FormationFilter ff)
+                                                                      PruneParams pp, u32 *err, FormationFilter ff,
+                                                                      CanonPlan plan)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 scan_scratch[33];
     __shared__ u64 base_sh;
-    stage_table(smem, g_move, g_ok);
-    const RowTable t{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    stage_table(smem, g_move);
+    const RowTable t{(const unsigned short *)smem};
     const u64 stride = (u64)gridDim.x * EXP_THREADS;
     for (u64 first = (u64)blockIdx.x * EXP_THREADS; first < n; first += stride) {
         const u64 idx = first + threadIdx.x;
@@ -116,12 +125,13 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
                 // a move that merges nothing keeps the multiset of tiles, so it keeps
                 // the input's (passing) prune verdict; merges show as new empty cells
                 const int empties = pp.enabled ? popc64(empty_mask(b)) : 0;
+                const bool planned = fixed_pattern(b) == plan.mask;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     u64 m;
                     if (move_left(t, v[k], &m) == 2 &&
                         !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
-                        r[k] = canonical(m);
+                        r[k] = canon_cand(m, planned ? plan.view[k] : 0xFFu);
                         mask |= 1u << k;
                     }
                 }
@@ -156,7 +166,7 @@ __global__ void __launch_bounds__(256) count_spawns_kernel(const u64 *__restrict
 
 __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restrict__ in, u64 n,
                                                             u64 *__restrict__ out2, u64 *__restrict__ out4,
-                                                            u64 cap, u64 *out_count, u32 *err)
+                                                            u64 cap, u64 *out_count, u32 *err, CanonPlan plan)
 {
     __shared__ u32 scan_scratch[33];
     __shared__ u64 base_sh;
@@ -174,9 +184,12 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
         if (pos + cnt > cap) {
             if (cnt) atomicOr(err, ERR_CAPACITY);
         } else {
-            // the images of b once; a spawn adds one nibble to each image
+            // the images of b once; a spawn adds one nibble to each image.  A spawn
+            // keeps b's 0xf cells, so only the plan's images of view 0 can be the
+            // maximum when b has the plan's mask
             u64 im[8];
             images(b, im);
+            const u32 cand = fixed_pattern(b) == plan.mask ? plan.view[0] : 0xFFu;
             while (e) {
                 const int bit = 63 - __clzll(e);  // nibble's low bit
                 e &= ~(1ull << bit);
@@ -184,6 +197,7 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
                 u64 m2 = 0, m4 = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
+                    if (!((cand >> k) & 1u)) continue;
                     const int sh = 60 - 4 * image_cell(k, cell);
                     m2 = umax64(m2, im[k] | (1ull << sh));
                     m4 = umax64(m4, im[k] | (2ull << sh));
@@ -243,7 +257,7 @@ static bool check(Counters &c, cudaStream_t s, const char *what)
 }
 
 bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const DeviceRowTable &t,
-                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff)
+                  const PruneParams &p, Counters &c, cudaStream_t s, FormationFilter ff, const CanonPlan &plan)
 {
     *n_out = 0;
     if (n == 0) return true;
@@ -259,7 +273,7 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
     kclock().begin(s, &kstats().expand_ms);
-    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, t.ok, p, c.err, ff);
+    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, p, c.err, ff, plan);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;
@@ -284,7 +298,8 @@ bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s)
     return true;
 }
 
-bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c, cudaStream_t s)
+bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c, cudaStream_t s,
+                   const CanonPlan &plan)
 {
     *n_out = 0;
     if (n == 0) return true;
@@ -292,7 +307,7 @@ bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_o
     if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
     const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
     kclock().begin(s, &kstats().spawn_ms);
-    expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err);
+    expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err, plan);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_count_checked(n_out, c, 0, s, "expand_spawns")) return false;

@@ -871,6 +871,8 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
     };
     Lay t2, t4, cur;
     FileWriter writer(3);
+    cgb::CanonPlan plan;
+    bool have_plan = false;
     for (unsigned i = start; i >= end && i; i -= 2) {
         const std::string bname = fmt_layer(posfmt, i);
         static_arr_info keys = read_boards(bname.c_str());
@@ -881,10 +883,15 @@ void solve(unsigned start, unsigned end, char *posfmt, char *tablefmt, const sta
             die("solve");
         if (cur.n && !CGB_CUDA(cudaMemcpyAsync(cur.keys, keys.bp, cur.n * 8, cudaMemcpyHostToDevice, st)))
             die("solve");
+        // the images that can be canonical follow the 0xf mask of the layer's boards
+        if (!have_plan && cur.n) {
+            plan = cgb::make_canon_plan(keys.bp[0], current_rules().free_formation != 0);
+            have_plan = true;
+        }
         const bool ok = vb == 4 ? cgb::solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, rules, e.rt,
-                                                        e.ctr, st)
+                                                        e.ctr, st, plan)
                                 : cgb::solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, rules, e.rt,
-                                                        e.ctr, st);
+                                                        e.ctr, st, plan);
         if (!ok) die("solve");
         // the values go to a pinned buffer on the I/O stream; the writer thread
         // writes the table (keys from the .boards file, values widened to f64

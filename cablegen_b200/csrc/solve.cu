@@ -9,8 +9,10 @@
 //     each successor looked up, canonicalised, in the s+2 / s+4 table; a miss
 //     is 0.0 (src/solve.c:108-164).  res = 0.9*S2/k + 0.1*S4/k.
 //
-// Work is compacted per warp: only legal moves are canonicalised and probed
-// (see solve_kernel).
+// Two kernels: solve_items_kernel (the default) spreads the (board, empty
+// cell) pairs of 32 boards over a warp's lanes; solve_direct_kernel runs one
+// thread per board.  Canonical forms take the maximum over the images a
+// CanonPlan allows for the board's 0xf mask (all eight without a plan).
 //
 // FP64 evaluates exactly the reference's operation sequence with
 // round-to-nearest intrinsics (no FMA contraction): bit-identical values.
@@ -29,9 +31,7 @@
 
 namespace cgb {
 
-constexpr int SOLVE_THREADS = 512;
-constexpr int SOLVE_SMEM = 65536 * 2 + 2048 * 4 + (512 / 32) * 2 * 128 * 8 * 2;
-constexpr int TABLE_BYTES_S = 65536 * 2 + 2048 * 4;
+constexpr int TABLE_BYTES_S = 65536 * 2;  // left-move rows, ROW_LOCKED for locked ones
 
 // ---- lookup ---------------------------------------------------------------
 template <typename V>
@@ -142,131 +142,129 @@ __device__ __forceinline__ void stage_table_s(unsigned char *smem, const unsigne
     __syncthreads();
 }
 
-// Each warp solves 32 boards at a time.  Every round takes the next empty
-// cell of each lane's board, forms the (up to) 8 moved successors of the two
-// spawns from the board's four move views (computed once per board), and
-// appends the legal ones to a per-warp queue in shared memory.  The warp then
-// canonicalises and looks up the queued boards 32 at a time -- only legal
-// moves cost a canonical form and a probe -- and each lane folds its best
-// values into its sums in cell order.
-constexpr int SOLVE_Q = 128;  // queue entries per spawn per warp (32 lanes x 4 moves)
+// Spawn-weighted mean of one board from its per-cell best values, in cell
+// order (src/solve.c:257-281): FP64 adds in order, FP32 Kahan-compensated sums;
+// the weighted mean is formed in FP64 and rounded once.
+template <typename V>
+struct SpawnSums {
+    V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
+    __device__ __forceinline__ void add(V best2, V best4)
+    {
+        if constexpr (sizeof(V) == 8) {  // cell order, plain IEEE adds
+            s2 = __dadd_rn(s2, best2);
+            s4 = __dadd_rn(s4, best4);
+        } else {  // Kahan-compensated
+            const float y2 = __fsub_rn(best2, c2), u2 = __fadd_rn(s2, y2);
+            c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
+            s2 = u2;
+            const float y4 = __fsub_rn(best4, c4), u4 = __fadd_rn(s4, y4);
+            c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
+            s4 = u4;
+        }
+    }
+    __device__ __forceinline__ V result(int spaces, u64 b, const SolveRules &r) const
+    {
+        double d = 0.0;
+        if (spaces) {
+            const double k = (double)spaces;
+            const double S2 = (double)s2 - (double)c2, S4 = (double)s4 - (double)c4;
+            d = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, S2), k), __ddiv_rn(__dmul_rn(0.1, S4), k));
+        }
+        if (r.score && d == 0.0) d = (double)tile_sum(b);
+        return (V)d;
+    }
+};
+
+// Item form: the work of a warp is its boards' (board, empty cell) pairs, not
+// its boards.  Boards have 0..16 empty cells, so one thread per board leaves a
+// warp waiting on its fullest board; here the 32 lanes take the pairs of 32
+// boards 32 at a time, every lane busy except in the last round.  A pair forms
+// the eight successors of its cell (2 spawns x 4 moves, from the owner's four
+// views), canonicalises them over the images its CanonPlan allows, probes the
+// s+2 and s+4 tables, and leaves the two best values in shared memory; the
+// owning lane then adds its pairs' values in cell order.
+constexpr int ITEM_THREADS = 1024;
+constexpr int ITEM_WARPS = ITEM_THREADS / 32;
+constexpr int ITEM_MAX = 32 * 16;  // pairs of 32 boards at most
+template <typename V>
+constexpr int item_smem() { return TABLE_BYTES_S + ITEM_WARPS * (ITEM_MAX * 2 + 2 * 32 * (int)sizeof(V)); }
 
 template <typename V>
-__global__ void __launch_bounds__(SOLVE_THREADS, 1) solve_kernel(const u64 *__restrict__ keys, u64 n,
-                                                                 V *__restrict__ out, DevTable<V> t2,
-                                                                 DevTable<V> t4, SolveRules r,
-                                                                 const unsigned short *g_move, u64 *probes_out)
+__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out);
+
+template <typename V>
+__global__ void __launch_bounds__(ITEM_THREADS, 1)
+    solve_items_kernel(const u64 *__restrict__ keys, u64 n, V *__restrict__ out, DevTable<V> t2, DevTable<V> t4,
+                       SolveRules r, const unsigned short *g_move, u64 *probes_out, CanonPlan plan)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
-    const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    const RowTable rt{(const unsigned short *)smem};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    u64 *qk = (u64 *)(smem + TABLE_BYTES_S) + (u64)warp * (2 * SOLVE_Q);                     // [2][Q] boards
-    V *qv = (V *)(smem + TABLE_BYTES_S + (SOLVE_THREADS / 32) * 2 * SOLVE_Q * 8) + warp * (2 * SOLVE_Q);
+    unsigned short *items = (unsigned short *)(smem + TABLE_BYTES_S) + warp * ITEM_MAX;  // (lane << 4) | cell
+    V *best_sh = (V *)(smem + TABLE_BYTES_S + ITEM_WARPS * ITEM_MAX * 2) + warp * 64;   // [2][32]
     u32 probes = 0;
-    const u64 stride = (u64)gridDim.x * SOLVE_THREADS;
-    for (u64 base = (u64)blockIdx.x * SOLVE_THREADS + warp * 32; base < n; base += stride) {
+    const u64 stride = (u64)gridDim.x * ITEM_THREADS;
+    for (u64 base = (u64)blockIdx.x * ITEM_THREADS + warp * 32; base < n; base += stride) {
         const u64 i = base + lane;
         const bool active = i < n;
         const u64 b = active ? keys[i] : 0;
         const bool sat = active && satisfied(b, r);
         u64 e = (active && !sat) ? empty_mask(b) : 0;
         const int spaces = popc64(e);
-        u64 v[4];
-        views(b, v);
-        V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
-        while (__any_sync(0xffffffffu, e != 0)) {
-            u64 m2[4], m4[4];
-            u32 l2 = 0, l4 = 0;
-            const bool has = e != 0;
+        const u32 inc = warp_inclusive_scan((u32)spaces);
+        const u32 off = inc - (u32)spaces;
+        const u32 total = __shfl_sync(0xffffffffu, inc, 31);
+        // this board's pairs, cells in order 0..15 (highest nibble first)
+        for (u32 j = off; e; j++) {
+            const int bit = 63 - __clzll(e);
+            e &= ~(1ull << bit);
+            items[j] = (unsigned short)((lane << 4) | ((60 - bit) >> 2));
+        }
+        const bool planned = fixed_pattern(b) == plan.mask;
+        __syncwarp();
+        SpawnSums<V> sums;
+        for (u32 r0 = 0; r0 < total; r0 += 32) {
+            const u32 j = r0 + (u32)lane;
+            const bool has = j < total;
+            const u32 it = has ? items[j] : 0u;
+            const int owner = (int)(it >> 4), cell = (int)(it & 15u);
+            const u64 ob = __shfl_sync(0xffffffffu, b, owner);
+            const bool opl = __shfl_sync(0xffffffffu, planned, owner);
+            V best2 = 0, best4 = 0;
             if (has) {
-                const int bit = 63 - __clzll(e);
-                e &= ~(1ull << bit);
-                const int cell = (60 - bit) >> 2;
+                u64 v[4];
+                views(ob, v);
+                u64 k2[4], k4[4];
+                u32 l2 = 0, l4 = 0;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int sh = 60 - 4 * view_cell(k, cell);
-                    if (move_left(rt, v[k] | (1ull << sh), &m2[k]) == 2) l2 |= 1u << k;
-                    if (move_left(rt, v[k] | (2ull << sh), &m4[k]) == 2) l4 |= 1u << k;
+                    const u32 cand = opl ? plan.view[k] : 0xFFu;
+                    u64 m;
+                    if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
+                    k2[k] = canon_cand(m, cand);
+                    if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
+                    k4[k] = canon_cand(m, cand);
                 }
                 probes += __popc(l2) + __popc(l4);
+                V p2[4], p4[4];
+                probe4(t2, k2, l2, p2);
+                probe4(t4, k4, l4, p4);
+                best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
+                best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
             }
-            // append the legal successors to the warp's queues
-            const u32 n2 = __popc(l2), n4 = __popc(l4);
-            const u32 packed = n2 | (n4 << 16);
-            const u32 inc = warp_inclusive_scan(packed);
-            const u32 tot = __shfl_sync(0xffffffffu, inc, 31);
-            const u32 off2 = (inc - packed) & 0xFFFF, off4 = (inc - packed) >> 16;
-            const u32 tot2 = tot & 0xFFFF, tot4 = tot >> 16;
-            {
-                u32 j2 = off2, j4 = off4;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    if (l2 & (1u << k)) qk[j2++] = m2[k];
-                    if (l4 & (1u << k)) qk[SOLVE_Q + j4++] = m4[k];
-                }
-            }
+            best_sh[lane] = best2;
+            best_sh[32 + lane] = best4;
             __syncwarp();
-            const u32 tmax = tot2 > tot4 ? tot2 : tot4;
-            for (u32 q = lane; q < tmax; q += 32) {
-                const bool do2 = q < tot2, do4 = q < tot4;
-                const u64 k2 = do2 ? canonical(qk[q]) : 0;
-                const u64 k4 = do4 ? canonical(qk[SOLVE_Q + q]) : 0;
-                if (t2.kind == INDEX_HASH && t4.kind == INDEX_HASH) {
-                    // issue both first probes before resolving either
-                    const u64 sa = (do2 && t2.cap) ? home_slot(k2, t2.cap) : 0;
-                    const u64 sb = (do4 && t4.cap) ? home_slot(k4, t4.cap) : 0;
-                    const ulonglong2 ea = (do2 && t2.cap) ? __ldg(t2.slots + sa) : make_ulonglong2(0, 0);
-                    const ulonglong2 eb = (do4 && t4.cap) ? __ldg(t4.slots + sb) : make_ulonglong2(0, 0);
-                    if (do2)
-                        qv[q] = (ea.x == k2) ? from_bits<V>(ea.y) : (ea.x == 0 ? V(0) : hash_probe_rest(t2, k2, sa));
-                    if (do4)
-                        qv[SOLVE_Q + q] =
-                            (eb.x == k4) ? from_bits<V>(eb.y) : (eb.x == 0 ? V(0) : hash_probe_rest(t4, k4, sb));
-                } else {
-                    if (do2) qv[q] = table_value(t2, k2);
-                    if (do4) qv[SOLVE_Q + q] = table_value(t4, k4);
-                }
-            }
-            __syncwarp();
-            if (has) {
-                V best2 = 0, best4 = 0;
-                u32 j2 = off2, j4 = off4;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    if (l2 & (1u << k)) best2 = vmax(best2, qv[j2++]);
-                    if (l4 & (1u << k)) best4 = vmax(best4, qv[SOLVE_Q + j4++]);
-                }
-                if constexpr (sizeof(V) == 8) {  // cell order, plain IEEE adds
-                    s2 = __dadd_rn(s2, best2);
-                    s4 = __dadd_rn(s4, best4);
-                } else {  // Kahan-compensated
-                    const float y2 = __fsub_rn(best2, c2), u2 = __fadd_rn(s2, y2);
-                    c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
-                    s2 = u2;
-                    const float y4 = __fsub_rn(best4, c4), u4 = __fadd_rn(s4, y4);
-                    c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
-                    s4 = u4;
-                }
-            }
+            // the owner adds the pairs of this round that are its own, in cell order
+            const u32 lo = off > r0 ? off : r0;
+            const u32 hi = (off + (u32)spaces) < r0 + 32 ? off + (u32)spaces : r0 + 32;
+            for (u32 q = lo; q < hi; q++) sums.add(best_sh[q - r0], best_sh[32 + q - r0]);
             __syncwarp();
         }
-        if (active) {
-            V res;
-            if (sat) {
-                res = V(1);
-            } else {
-                double d = 0.0;
-                if (spaces) {
-                    const double k = (double)spaces;
-                    const double S2 = (double)s2 - (double)c2, S4 = (double)s4 - (double)c4;
-                    d = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, S2), k), __ddiv_rn(__dmul_rn(0.1, S4), k));
-                }
-                if (r.score && d == 0.0) d = (double)tile_sum(b);
-                res = (V)d;
-            }
-            out[i] = res;
-        }
+        if (active) out[i] = sat ? V(1) : sums.result(spaces, b, r);
+        __syncwarp();
     }
     add_probes(probes, probes_out);
 }
@@ -306,11 +304,11 @@ __global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u
                                                                          V *__restrict__ out, DevTable<V> t2,
                                                                          DevTable<V> t4, SolveRules r,
                                                                          const unsigned short *g_move,
-                                                                         u64 *probes_out)
+                                                                         u64 *probes_out, CanonPlan plan)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     stage_table_s(smem, g_move);
-    const RowTable rt{(const unsigned short *)smem, (const u32 *)(smem + 65536 * 2)};
+    const RowTable rt{(const unsigned short *)smem};
     u32 probes = 0;
     for (u64 i = (u64)blockIdx.x * DIRECT_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * DIRECT_THREADS) {
         const u64 b = keys[i];
@@ -322,7 +320,8 @@ __global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u
             const int spaces = popc64(e);
             u64 v[4];
             views(b, v);
-            V s2 = 0, s4 = 0, c2 = 0, c4 = 0;
+            const bool planned = fixed_pattern(b) == plan.mask;
+            SpawnSums<V> sums;
             while (e) {  // cells in order 0..15 = highest nibble first
                 const int bit = 63 - __clzll(e);
                 e &= ~(1ull << bit);
@@ -332,38 +331,20 @@ __global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int sh = 60 - 4 * view_cell(k, cell);
+                    const u32 cand = planned ? plan.view[k] : 0xFFu;
                     u64 m;
                     if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
-                    k2[k] = canonical(m);
+                    k2[k] = canon_cand(m, cand);
                     if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
-                    k4[k] = canonical(m);
+                    k4[k] = canon_cand(m, cand);
                 }
                 probes += __popc(l2) + __popc(l4);
                 V p2[4], p4[4];
                 probe4(t2, k2, l2, p2);
                 probe4(t4, k4, l4, p4);
-                const V best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
-                const V best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
-                if constexpr (sizeof(V) == 8) {
-                    s2 = __dadd_rn(s2, best2);
-                    s4 = __dadd_rn(s4, best4);
-                } else {
-                    const float y2 = __fsub_rn(best2, c2), u2 = __fadd_rn(s2, y2);
-                    c2 = __fsub_rn(__fsub_rn(u2, s2), y2);
-                    s2 = u2;
-                    const float y4 = __fsub_rn(best4, c4), u4 = __fadd_rn(s4, y4);
-                    c4 = __fsub_rn(__fsub_rn(u4, s4), y4);
-                    s4 = u4;
-                }
+                sums.add(vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3])), vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3])));
             }
-            double d = 0.0;
-            if (spaces) {
-                const double k = (double)spaces;
-                const double S2 = (double)s2 - (double)c2, S4 = (double)s4 - (double)c4;
-                d = __dadd_rn(__ddiv_rn(__dmul_rn(0.9, S2), k), __ddiv_rn(__dmul_rn(0.1, S4), k));
-            }
-            if (r.score && d == 0.0) d = (double)tile_sum(b);
-            res = (V)d;
+            res = sums.result(spaces, b, r);
         }
         out[i] = res;
     }
@@ -503,16 +484,16 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     return t;
 }
 
-int g_solve_variant = 0;  // 0: direct (one thread per board), 1: warp-compacted queue
+int g_solve_variant = 1;  // 0: direct (one thread per board), 1: (board, cell) pairs per warp
 
 static bool solve_attrs()
 {
     static bool attr = false;
     if (!attr) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           SOLVE_SMEM)) ||
-            !CGB_CUDA(cudaFuncSetAttribute(solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           SOLVE_SMEM)) ||
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           item_smem<double>())) ||
+            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           item_smem<float>())) ||
             !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<double>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_BYTES_S)) ||
             !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<float>,
@@ -526,25 +507,27 @@ static bool solve_attrs()
 // the kernel launch alone: no host round trip, so it may be captured in a graph
 template <class V>
 static void enqueue_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
-                          const SolveRules &r, const DeviceRowTable &rt, u64 *probes, cudaStream_t s)
+                          const SolveRules &r, const DeviceRowTable &rt, u64 *probes, cudaStream_t s,
+                          const CanonPlan &plan)
 {
     if (g_solve_variant == 1)
-        solve_kernel<V><<<grid_for(n, SOLVE_THREADS, 1), SOLVE_THREADS, SOLVE_SMEM, s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes);
+        solve_items_kernel<V><<<grid_for(n, ITEM_THREADS, 1), ITEM_THREADS, item_smem<V>(), s>>>(
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
     else
         solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes);
+            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
 }
 
 template <class V>
 static bool launch_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, const LayerIndex &t4,
-                         const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
+                         const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s,
+                         const CanonPlan &plan)
 {
     if (n == 0) return true;
     if (!solve_attrs()) return false;
     if (!CGB_CUDA(cudaMemsetAsync(c.d + 2, 0, sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().solve_ms);
-    enqueue_solve<V>(keys, n, out, t2, t4, r, rt, c.d + 2, s);
+    enqueue_solve<V>(keys, n, out, t2, t4, r, rt, c.d + 2, s, plan);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u64 probes = 0;
@@ -565,8 +548,8 @@ bool solve_layer_enqueue(const u64 *keys, u64 n, void *out, int vbytes, const La
 {
     if (n == 0) return true;
     if (!solve_attrs()) return false;
-    if (vbytes == 4) enqueue_solve<float>(keys, n, (float *)out, t2, t4, r, rt, probes, s);
-    else enqueue_solve<double>(keys, n, (double *)out, t2, t4, r, rt, probes, s);
+    if (vbytes == 4) enqueue_solve<float>(keys, n, (float *)out, t2, t4, r, rt, probes, s, CanonPlan{});
+    else enqueue_solve<double>(keys, n, (double *)out, t2, t4, r, rt, probes, s, CanonPlan{});
     KernelStats &k = kstats();
     k.solve_launches++;
     k.solve_boards += n;
@@ -607,15 +590,15 @@ bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *e
 }
 
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,
-                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s, const CanonPlan &plan)
 {
-    return launch_solve<double>(keys, n, out, t2, t4, r, rt, c, s);
+    return launch_solve<double>(keys, n, out, t2, t4, r, rt, c, s, plan);
 }
 
 bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, const LayerIndex &t4,
-                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s)
+                     const SolveRules &r, const DeviceRowTable &rt, Counters &c, cudaStream_t s, const CanonPlan &plan)
 {
-    return launch_solve<float>(keys, n, out, t2, t4, r, rt, c, s);
+    return launch_solve<float>(keys, n, out, t2, t4, r, rt, c, s, plan);
 }
 
 }  // namespace cgb

@@ -165,8 +165,9 @@ struct Chain {
         cur.vb = layer_vbytes(cur.sum);
         if (cur.vb == 4 && !(narrow(e, t2, s) && narrow(e, t4, s))) return false;
         if (!dev_alloc(&cur.vals, cur.n * cur.vb + 8, s)) return false;
-        if (cur.vb == 4) return solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
-        return solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s);
+        if (cur.vb == 4)
+            return solve_layer_f32(cur.keys, cur.n, (float *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s, e.plan);
+        return solve_layer_f64(cur.keys, cur.n, (double *)cur.vals, t2.ix, t4.ix, r, e.rt, e.ctr, s, e.plan);
     }
     bool index(Engine &e, cudaStream_t s)
     {

@@ -319,11 +319,19 @@ extern "C" int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, 
     bool ok = build_index(t2, E().index_kind, vb, st2, E().bucket_bits, E().ctr, s) &&
               build_index(t4, E().index_kind, vb, st4, E().bucket_bits, E().ctr, s);
     const SolveRules r = make_solve_rules(E().rules, d_ws, (int)ws.size());
+    // the images that can be canonical follow the 0xf mask of the first board
+    CanonPlan plan;
+    if (ok && n) {
+        u64 first = 0;
+        ok = CGB_CUDA(cudaMemcpyAsync(&first, d_keys, 8, cudaMemcpyDeviceToHost, s)) &&
+             CGB_CUDA(cudaStreamSynchronize(s));
+        plan = make_canon_plan(first, E().rules.free_formation != 0);
+    }
     if (ok) {
         if (precision == 32)
-            ok = solve_layer_f32(d_keys, n, (float *)d_out, t2, t4, r, E().rt, E().ctr, s);
+            ok = solve_layer_f32(d_keys, n, (float *)d_out, t2, t4, r, E().rt, E().ctr, s, plan);
         else
-            ok = solve_layer_f64(d_keys, n, (double *)d_out, t2, t4, r, E().rt, E().ctr, s);
+            ok = solve_layer_f64(d_keys, n, (double *)d_out, t2, t4, r, E().rt, E().ctr, s, plan);
     }
     dev_free(d_ws, s);
     dev_free(st2.p, s);
