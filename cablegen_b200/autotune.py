@@ -4,8 +4,11 @@ The knobs (cgb_set_option):
 
 * ``sort_variant``  -- the digit pass of the radix sort: 0 ranks a 4096-key tile with warp
   match, 1 with eight ballots per digit (keys re-read from L2 for the local scatter), 2 keeps
-  persistent CTAs that bulk-copy the next tile into shared memory while ranking the current one;
-* ``solve_variant`` -- 0 one thread per board, 1 warp-compacted successor queue;
+  persistent CTAs that bulk-copy the next tile into shared memory while ranking the current one,
+  3 is the ballot pass specialised for byte digits (full tiles without bounds tests, digits read
+  from the one 32-bit word that holds them);
+* ``solve_variant`` -- 0 one thread per board, 1 the (board, empty cell) pairs of 32 boards
+  spread over a warp;
 * ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
   table size; a higher load means more probes, a lower one more memory and a lower L2 hit
   rate).
@@ -27,8 +30,8 @@ from typing import Dict, Optional
 from . import configs, device
 
 KNOBS = {
-    "sort_variant": [1, 0, 2],
-    "solve_variant": [0, 1],
+    "sort_variant": [3, 1, 0, 2],
+    "solve_variant": [1, 0],
     "hash_load_pct": [0, 25, 45],
 }
 
@@ -81,8 +84,9 @@ def tune(workload: str = "batch64", end_cap: int = 300, precision: int = 32, rep
     best_ms = measure()
     trials.append({"params": dict(params), "ms": best_ms})
     for knob, values in KNOBS.items():
+        start = params[knob]  # measured already, with the other knobs as they are now
         for v in values:
-            if v == params[knob]:
+            if v == start:
                 continue
             device.set_option(knob, v)
             ms = measure()

@@ -348,6 +348,129 @@ __global__ void __launch_bounds__(SORT_THREADS, 5)
 }
 
 // ---------------------------------------------------------------------------
+// Third form of the ballot pass, for byte digits of the key: the tile's body
+// is specialised for full tiles (no bounds tests on 4095 of every 4096 keys),
+// the ranking phase reads only the 32-bit word that holds the digit, digits
+// come out of words with one byte permute, and each bin keeps one combined
+// offset (global start - local start) for the final write.
+template <bool FULL>
+__device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
+                                               const u32 *__restrict__ digit_hist, u32 *lookback, u32 tile, u32 *err,
+                                               u64 *keys_sh, u32 (*warp_hist)[RADIX], u32 *bin_local, u32 *bin_delta,
+                                               u32 *scan_scratch)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 tile_base = tile * BAL_TILE;
+    const u32 warp_base = tile_base + warp * (BAL_KPT * 32);
+    const u32 *src_w = (const u32 *)src + (shift >= 32 ? 1 : 0);   // little-endian words of the keys
+    const u32 sel = 0x4440u | (u32)((shift >> 3) & 3);              // the digit's byte, zero above it
+    u32 dg[BAL_KPT / 4];
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        const u32 dd = (FULL || idx < n) ? __byte_perm(__ldg(src_w + 2 * (u64)idx), 0, sel) : 0u;
+        if (i % 4 == 0) dg[i / 4] = dd;
+        else dg[i / 4] |= dd << (8 * (i % 4));
+    }
+    const u32 lt = lanemask_lt();
+    u32 rank2[BAL_KPT / 2];
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 d = __byte_perm(dg[i / 4], 0, 0x4440u | (u32)(i % 4));
+        u32 peers;
+        if (FULL) {
+            peers = 0xffffffffu;
+        } else {
+            const u32 idx = warp_base + i * 32 + lane;
+            peers = __ballot_sync(0xffffffffu, idx < n);
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const u32 bj = __ballot_sync(0xffffffffu, (d >> j) & 1);
+            peers &= ((d >> j) & 1) ? bj : ~bj;
+        }
+        const u32 base = warp_hist[warp][d];   // every peer reads the same word
+        __syncwarp();
+        const bool leader = (peers & lt) == 0;
+        if (FULL) {
+            if (leader) warp_hist[warp][d] = base + __popc(peers);
+        } else {
+            const u32 idx = warp_base + i * 32 + lane;
+            if (idx < n && leader) warp_hist[warp][d] = base + __popc(peers);
+        }
+        __syncwarp();
+        const u32 r = base + __popc(peers & lt);
+        if (i & 1) rank2[i >> 1] |= r << 16;
+        else rank2[i >> 1] = r;
+    }
+    __syncthreads();
+    const u32 d = threadIdx.x;  // SORT_THREADS == RADIX
+    u32 cnt = 0;
+#pragma unroll
+    for (int w = 0; w < SORT_THREADS / 32; w++) {
+        const u32 c = warp_hist[w][d];
+        warp_hist[w][d] = cnt;
+        cnt += c;
+    }
+    u32 *lb = lookback + (u64)tile * RADIX + d;
+    if (tile != 0 || !g_hold_first_tile) st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
+    u32 total;
+    const u32 lstart = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
+    bin_local[d] = lstart;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < BAL_KPT; i++) {
+        const u32 idx = warp_base + i * 32 + lane;
+        if (FULL || idx < n) {
+            const u64 key = src[idx];
+            const u32 dd = __byte_perm(dg[i / 4], 0, 0x4440u | (u32)(i % 4));
+            const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xFFFF;
+            keys_sh[bin_local[dd] + warp_hist[warp][dd] + r] = key;
+        }
+    }
+    u32 excl = 0;
+    if (tile != 0) {
+        excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
+        st_relaxed(lb, LB_PRE | (excl + cnt));
+    }
+    const u32 gexcl = block_exclusive_scan<u32>(digit_hist[d], scan_scratch, &total);
+    bin_delta[d] = gexcl + excl - lstart;
+    __syncthreads();
+    const bool hiw = shift >= 32;
+    const u32 tile_n = FULL ? (u32)BAL_TILE : min((u32)BAL_TILE, n - tile_base);
+#pragma unroll 4
+    for (u32 j = threadIdx.x; j < tile_n; j += SORT_THREADS) {
+        const u64 key = keys_sh[j];
+        const u32 dd = __byte_perm(hiw ? (u32)(key >> 32) : (u32)key, 0, sel);
+        const u32 g = bin_delta[dd] + j;
+        if (g < n) dst[g] = key;
+        else atomicOr(err, ERR_CAPACITY);
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS, 5)
+    onesweep_byte_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
+                         const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err)
+{
+    __shared__ u64 keys_sh[BAL_TILE];
+    __shared__ u32 warp_hist[SORT_THREADS / 32][RADIX];
+    __shared__ u32 bin_local[RADIX];
+    __shared__ u32 bin_delta[RADIX];
+    __shared__ u32 scan_scratch[33];
+    __shared__ u32 tile_sh;
+    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < (SORT_THREADS / 32) * RADIX; i += SORT_THREADS) (&warp_hist[0][0])[i] = 0;
+    __syncthreads();
+    const u32 tile = tile_sh;
+    if ((u64)(tile + 1) * BAL_TILE <= n)
+        byte_pass_tile<true>(src, dst, n, shift, digit_hist, lookback, tile, err, keys_sh, warp_hist, bin_local,
+                             bin_delta, scan_scratch);
+    else
+        byte_pass_tile<false>(src, dst, n, shift, digit_hist, lookback, tile, err, keys_sh, warp_hist, bin_local,
+                              bin_delta, scan_scratch);
+}
+
+// ---------------------------------------------------------------------------
 // Persistent, software-pipelined digit pass.  Each CTA loops over tiles taken
 // in order from the tile counter; while it ranks and scatters tile t, the
 // bulk-copy engine already loads tile t+1 into the CTA's second shared
@@ -514,7 +637,7 @@ static int pipe_grid(int device)
     return grid;
 }
 
-int g_sort_variant = 1;  // 0: match-based ranking, 1: ballot-based ranking, 2: pipelined persistent
+int g_sort_variant = 3;  // 0: match ranking, 1: ballot ranking, 2: pipelined persistent, 3: byte-digit ballot
 
 // test switches of the look-back waits (see g_spin_limit); 0 restores the default limit
 bool set_lookback_test(u32 spin_limit, int hold_first_tile)
@@ -855,7 +978,7 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         pgrid = pipe_grid(dev);
         if (pgrid <= 0 || (((uintptr_t)keys | (uintptr_t)tmp) & 15)) variant = 1;
     }
-    const u32 pass_tiles = variant == 2 ? ceil_div(n, PIPE_TILE) : variant == 1 ? ceil_div(n, BAL_TILE) : tiles;
+    const u32 pass_tiles = variant == 2 ? ceil_div(n, PIPE_TILE) : (variant == 1 || variant == 3) ? ceil_div(n, BAL_TILE) : tiles;
     u64 *src = keys, *dst = tmp;
     for (int p = 0; p < np; p++) {
         const int d = digits[p];
@@ -869,6 +992,11 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
             onesweep_ballot_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, ShiftDigit{8 * d},
                                                                   ws.small + W_HIST + d * RADIX, ws.lookback,
                                                                   ws.small + W_CTR + p, ws.small + W_ERR);
+        else if (variant == 3)
+            onesweep_byte_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d,
+                                                                                ws.small + W_HIST + d * RADIX,
+                                                                                ws.lookback, ws.small + W_CTR + p,
+                                                                                ws.small + W_ERR);
         else
             onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
                                                            ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);

@@ -97,13 +97,14 @@ int cgb_set_option(const char *name, long long value)
         E().index_kind = (int)value;
     } else if (k == "solve_variant") {
         if (value < 0 || value > 1) {
-            set_error("cgb_set_option: solve_variant must be 0 (direct) or 1 (warp queue)");
+            set_error("cgb_set_option: solve_variant must be 0 (one thread per board) or 1 (board-cell pairs)");
             return -1;
         }
         g_solve_variant = (int)value;
     } else if (k == "sort_variant") {
-        if (value < 0 || value > 2) {
-            set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking) or 2 (pipelined)");
+        if (value < 0 || value > 3) {
+            set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking), 2 (pipelined) "
+                      "or 3 (byte-digit ballot ranking)");
             return -1;
         }
         g_sort_variant = (int)value;

@@ -77,19 +77,20 @@ def test_output_one_short_is_reported(cuda):
     cuda.set_rules(w.settings)
     x = cuda.to_device(realistic_boards(np.random.default_rng(4), 100_000))
     L = _lib.lib()
-    need = cuda.expand_moves(x).numel()
-    out = torch.full((need + 8,), -1, dtype=torch.int64, device="cuda")
+    total = cuda.count_spawns(x)
+    o2 = torch.full((total + 8,), -1, dtype=torch.int64, device="cuda")
+    o4 = torch.full((total + 8,), -1, dtype=torch.int64, device="cuda")
     cnt = C.c_uint64()
     torch.cuda.synchronize()
-    assert L.cgb_expand_moves(x.data_ptr(), x.numel(), out.data_ptr(), need - 1, C.byref(cnt)) == -1
-    assert "output capacity exceeded" in L.cgb_last_error().decode()
-    assert int(out[need - 1]) == -1            # nothing written past the capacity
-    total = cuda.count_spawns(x)
-    o2 = torch.empty(total, dtype=torch.int64, device="cuda")
-    o4 = torch.empty(total, dtype=torch.int64, device="cuda")
     assert L.cgb_expand_spawns(x.data_ptr(), x.numel(), o2.data_ptr(), o4.data_ptr(), total - 1, C.byref(cnt)) == -1
     assert "output capacity exceeded" in L.cgb_last_error().decode()
-    assert cuda.expand_moves(x).numel() == need   # and the next call works
+    assert int(o2[total - 1]) == -1 and int(o4[total - 1]) == -1   # nothing written past the capacity
+    # the move expansion refuses an output below its 4n bound before launching
+    out = torch.empty(4 * x.numel(), dtype=torch.int64, device="cuda")
+    assert L.cgb_expand_moves(x.data_ptr(), x.numel(), out.data_ptr(), 4 * x.numel() - 1, C.byref(cnt)) == -1
+    assert "4n" in L.cgb_last_error().decode()
+    got2, got4 = cuda.expand_spawns(x)                # and the next call works
+    assert got2.numel() == total and got4.numel() == total
 
 
 def test_capped_allocator_engine_call_fails_cleanly(cuda):
