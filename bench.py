@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--case", default=None, choices=["sort", "expand", "solve"],
                     help="one small kernel case for a profiler capture instead of the benchmark")
     ap.add_argument("--case-end", type=int, default=260, help="end tile sum of the solve case")
+    ap.add_argument("--set", action="append", default=[], metavar="NAME=VALUE",
+                    help="engine option (cgb_set_option) applied before the runs; repeatable")
     return ap.parse_args()
 
 
@@ -343,6 +345,9 @@ def run_ours(args):
     form = wl.formations[0]
     device.init(dev)
     device.set_rules(wl.settings)
+    for kv in args.set:
+        k, v = kv.split("=", 1)
+        device.set_option(k, int(v))
 
     def step(precision=64, e2e=False):
         h = {"d2h": 0}
@@ -600,6 +605,9 @@ def run_case(args):
     device.init(0)
     w = configs.get("ll_pruned")
     device.set_rules(w.settings)
+    for kv in args.set:
+        k, v = kv.split("=", 1)
+        device.set_option(k, int(v))
     rng = np.random.default_rng(5)
     if args.case == "sort":
         c = device.canonicalize(device.to_device(random_ll_boards(rng, 25_000_000)))

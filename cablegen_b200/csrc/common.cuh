@@ -45,6 +45,7 @@ struct KernelStats {
     u64 hist_bytes = 0, onesweep_bytes = 0, unique_bytes = 0, merge_bytes = 0, expand_bytes = 0,
         spawn_bytes = 0, solve_bytes = 0;
     u64 onesweep_launches = 0, solve_launches = 0, solve_boards = 0, lookups = 0;
+    u64 index_builds = 0, compact_index_builds = 0;
 };
 KernelStats &kstats();
 

@@ -6,6 +6,7 @@
 #include <vector>
 #include "common.cuh"
 #include "board.cuh"
+#include "hashidx.cuh"
 
 namespace cgb {
 
@@ -99,6 +100,7 @@ struct LayerIndex {
     // INDEX_HASH
     const void *slots = nullptr;  // cap slots of {u64 key, u64 value bits}; key 0 = empty
     u64 cap = 0;
+    CompactHash ch;               // ch.on: cap (a power of two) 8-byte slots instead
 };
 
 // device storage owned by one index (reused across layers)

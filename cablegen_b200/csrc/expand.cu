@@ -7,9 +7,10 @@
 // marked ROW_LOCKED) is staged into shared memory once per CTA of a
 // persistent grid; right/up/down reuse it through the board views of
 // board.cuh.  Canonical forms take the maximum over the images a CanonPlan
-// names for the board's 0xf mask (all eight without a plan).  Results are
-// appended with one atomic per CTA iteration after a block scan, so the
-// output is compact (no 4N slot array + separate scan).
+// names for the board's 0xf mask (all eight without a plan).  Repeated
+// results of one CTA iteration are dropped through a shared-memory set, and
+// the rest are appended with one atomic per CTA iteration after a block scan,
+// so the output is compact (no 4N slot array + separate scan).
 //
 // expand_spawns restates src/generate.c:177-199: every empty cell receives a
 // 2 (nibble 1) and a 4 (nibble 2); both boards are canonicalised.  The exact
@@ -99,6 +100,29 @@ __device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned 
     __syncthreads();
 }
 
+// Set of the move results of one CTA iteration (1024 input boards, at most
+// 4096 results) in shared memory: open addressing over 8192 u64 slots, 0 =
+// empty (no canonical board is 0).  Neighbouring boards of a sorted layer
+// often move to the same board (rows that differ only in where their tiles
+// sit before a slide), so dropping the repeats here keeps about half of the
+// raw move stream out of the sort (measured on LL layers: 1024 consecutive
+// inputs keep 53 % of their results).
+constexpr int MOVE_SET = 8192;
+constexpr int EXP_SMEM = TABLE_BYTES + MOVE_SET * 8;
+
+__device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
+{
+    u32 h = ((u32)(key >> 32) * 0x9E3779B1u) ^ ((u32)key * 0x85EBCA77u);
+    h ^= h >> 15;
+    for (u32 i = 0; i < MOVE_SET; i++) {
+        const u32 slot = (h + i) & (MOVE_SET - 1);
+        const unsigned long long prev = atomicCAS(set + slot, 0ull, (unsigned long long)key);
+        if (prev == 0ull) return true;   // first copy
+        if (prev == key) return false;   // a repeat
+    }
+    return true;  // unreachable: the set is never more than half full
+}
+
 __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
@@ -110,8 +134,11 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
     __shared__ u64 base_sh;
     stage_table(smem, g_move);
     const RowTable t{(const unsigned short *)smem};
+    unsigned long long *set = (unsigned long long *)(smem + TABLE_BYTES);
     const u64 stride = (u64)gridDim.x * EXP_THREADS;
     for (u64 first = (u64)blockIdx.x * EXP_THREADS; first < n; first += stride) {
+        for (int i = threadIdx.x; i < MOVE_SET; i += EXP_THREADS) set[i] = 0ull;
+        __syncthreads();
         const u64 idx = first + threadIdx.x;
         u64 r[4] = {0, 0, 0, 0};
         u32 mask = 0;
@@ -132,7 +159,7 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
                     if (move_left(t, v[k], &m) == 2 &&
                         !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
                         r[k] = canon_cand(m, planned ? plan.view[k] : 0xFFu);
-                        mask |= 1u << k;
+                        if (set_insert(set, r[k])) mask |= 1u << k;
                     }
                 }
             }
@@ -264,7 +291,7 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     static bool attr = false;
     if (!attr) {
         if (!CGB_CUDA(cudaFuncSetAttribute(expand_moves_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           TABLE_BYTES)))
+                                           EXP_SMEM)))
             return false;
         attr = true;
     }
@@ -273,7 +300,7 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
     kclock().begin(s, &kstats().expand_ms);
-    expand_moves_kernel<<<grid, EXP_THREADS, TABLE_BYTES, s>>>(in, n, out, cap, c.d, t.move, p, c.err, ff, plan);
+    expand_moves_kernel<<<grid, EXP_THREADS, EXP_SMEM, s>>>(in, n, out, cap, c.d, t.move, p, c.err, ff, plan);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;

@@ -45,6 +45,7 @@ struct DevTable {
     u64 prefix_value;
     const ulonglong2 *slots;
     u64 cap;
+    CompactHash ch;  // INDEX_HASH with 8-byte slots (ch.on)
 };
 
 template <typename V>
@@ -95,12 +96,35 @@ __device__ __noinline__ V hash_probe_rest(const DevTable<V> &t, u64 key, u64 s)
     return V(0);
 }
 
+// continue a compact probe after the home slot held another key
+template <typename V>
+__device__ __noinline__ V compact_probe_rest(const DevTable<V> &t, u64 home, u32 tag0)
+{
+    const u64 *w = (const u64 *)t.slots;
+    const u32 last = (1u << t.ch.dbits) - 1u;  // probe distances stay below it (the build checks)
+    for (u32 d = 1; d + 1 < last; d++) {
+        const u64 e = __ldg(w + ((home + d) & (t.cap - 1)));
+        if ((u32)e == tag0 + d) return from_bits<V>(e >> 32);
+        if ((u32)e == 0u) return V(0);
+    }
+    return V(0);
+}
+
 template <typename V>
 __device__ __forceinline__ V vmax(V a, V b) { return a > b ? a : b; }
 
 template <typename V>
 __device__ __forceinline__ V table_value(const DevTable<V> &t, u64 key)
 {
+    if (t.kind == INDEX_HASH && t.ch.on) {
+        if ((key & t.ch.cmask) != t.ch.cval) return V(0);
+        u32 tag0;
+        const u64 h = compact_home(t.ch, key, &tag0);
+        const u64 e = __ldg((const u64 *)t.slots + h);
+        if ((u32)e == tag0) return from_bits<V>(e >> 32);
+        if ((u32)e == 0u) return V(0);
+        return compact_probe_rest(t, h, tag0);
+    }
     if (t.kind == INDEX_HASH) {
         if (t.cap == 0) return V(0);
         const u64 s = home_slot(key, t.cap);
@@ -278,6 +302,23 @@ constexpr int DIRECT_THREADS = 1024;
 template <typename V>
 __device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out)
 {
+    if (t.kind == INDEX_HASH && t.ch.on) {
+        u64 h[4], e[4];
+        u32 tag[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && (key[j] & t.ch.cmask) == t.ch.cval;
+            h[j] = compact_home(t.ch, key[j], &tag[j]);
+            e[j] = on ? __ldg((const u64 *)t.slots + h[j]) : 0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((u32)e[j] == tag[j]) out[j] = from_bits<V>(e[j] >> 32);
+            else if ((u32)e[j] == 0u) out[j] = V(0);
+            else out[j] = compact_probe_rest(t, h[j], tag[j]);
+        }
+        return;
+    }
     if (t.kind == INDEX_HASH) {
         u64 s[4];
         ulonglong2 e[4];
@@ -385,6 +426,45 @@ __global__ void hash_build_kernel(const u64 *__restrict__ keys, const V *__restr
     }
 }
 
+__global__ void key_bits_kernel(const u64 *__restrict__ keys, u64 n, unsigned long long *and_or)
+{
+    u64 a = ~0ull, o = 0;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 k = keys[i];
+        a &= k;
+        o |= k;
+    }
+    for (int d = 16; d; d >>= 1) {
+        a &= __shfl_xor_sync(0xffffffffu, a, d);
+        o |= __shfl_xor_sync(0xffffffffu, o, d);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAnd(and_or, (unsigned long long)a);
+        atomicOr(and_or + 1, (unsigned long long)o);
+    }
+}
+
+__global__ void compact_build_kernel(const u64 *__restrict__ keys, const float *__restrict__ vals, u64 n,
+                                     unsigned long long *slots, CompactHash c, u64 cap, u32 *err)
+{
+    const u32 last = (1u << c.dbits) - 1u;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        u32 tag0;
+        const u64 h = compact_home(c, keys[i], &tag0);
+        const u64 vbits = (u64)__float_as_uint(vals[i]) << 32;
+        bool placed = false;
+        for (u32 d = 0; d + 1 < last; d++) {
+            const unsigned long long prev =
+                atomicCAS(slots + ((h + d) & (cap - 1)), 0ull, (unsigned long long)(vbits | (tag0 + d)));
+            if (prev == 0ull) {
+                placed = true;
+                break;
+            }
+        }
+        if (!placed) atomicOr(err, ERR_CAPACITY);  // the host falls back to 16-byte slots
+    }
+}
+
 static int grid_for(u64 n, int threads, int per_sm)
 {
     int dev = 0, sms = 0;
@@ -406,6 +486,48 @@ static bool ensure_storage(IndexStorage &st, u64 bytes, cudaStream_t s)
     return true;
 }
 
+int g_hash_compact = 1;  // FP32 hash tables in 8-byte slots where the keys allow it
+
+// plans and builds the 8-byte-slot index of an FP32 layer: AND/OR of the keys
+// give the constant bytes; the table is the power of two at or above twice the
+// layer; the tag holds the remainder bits (at most 26) and the probe distance.
+// Leaves ix.kind == INDEX_BISECT (nothing built) when the keys vary in too many
+// bytes or a key would sit further from home than the tag can say.
+static bool build_compact(LayerIndex &ix, IndexStorage &st, Counters &c, cudaStream_t s)
+{
+    unsigned long long init[2] = {~0ull, 0ull};
+    if (!CGB_CUDA(cudaMemcpyAsync(c.d + 3, init, 16, cudaMemcpyHostToDevice, s))) return false;
+    key_bits_kernel<<<grid_for(ix.n, 256, 8), 256, 0, s>>>(ix.keys, ix.n, (unsigned long long *)(c.d + 3));
+    u64 ao[2];
+    if (!CGB_CUDA(cudaGetLastError()) || !CGB_CUDA(cudaMemcpyAsync(ao, c.d + 3, 16, cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaStreamSynchronize(s)))
+        return false;
+    int cbits = 0;
+    const CompactHash ch = plan_compact(ao[0], ao[1], ix.n, &cbits);
+    if (!ch.on) return true;
+    const u64 cap = 1ull << cbits;
+    if (!ensure_storage(st, cap * 8, s)) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(st.p, 0, cap * 8, s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+    kclock().begin(s, &kstats().index_ms);
+    compact_build_kernel<<<grid_for(ix.n, 256, 16), 256, 0, s>>>(ix.keys, (const float *)ix.vals, ix.n,
+                                                                 (unsigned long long *)st.p, ch, cap, c.err);
+    kclock().end(s);
+    u32 e = 0;
+    if (!CGB_CUDA(cudaGetLastError()) || !CGB_CUDA(cudaMemcpyAsync(&e, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaStreamSynchronize(s)))
+        return false;
+    kclock().flush();
+    if (e) return true;  // a probe ran past what the tag can hold: 16-byte slots instead
+    ix.kind = INDEX_HASH;
+    ix.slots = st.p;
+    ix.cap = cap;
+    ix.ch = ch;
+    kstats().index_builds++;
+    kstats().compact_index_builds++;
+    return true;
+}
+
 bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
                  cudaStream_t s)
 {
@@ -414,6 +536,11 @@ bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int buc
     ix.slots = nullptr;
     ix.cap = 0;
     if (ix.n == 0 || kind == INDEX_BISECT) return true;
+    ix.ch = CompactHash{};
+    if (kind == INDEX_HASH && vbytes == 4 && g_hash_compact && ix.n >= 64) {
+        if (!build_compact(ix, st, c, s)) return false;
+        if (ix.kind == INDEX_HASH) return true;
+    }
     if (kind == INDEX_HASH) {
         // load factor <= g_hash_load_pct: capacity rounded up to a multiple of 64 slots
         const u64 cap = hash_capacity(ix.n);
@@ -440,6 +567,7 @@ bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int buc
         ix.kind = INDEX_HASH;
         ix.slots = st.p;
         ix.cap = cap;
+        kstats().index_builds++;
         return true;
     }
     // INDEX_BUCKET
@@ -481,6 +609,7 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     t.prefix_value = ix.prefix_value;
     t.slots = (const ulonglong2 *)ix.slots;
     t.cap = ix.kind == INDEX_HASH ? ix.cap : 0;
+    t.ch = ix.ch;
     return t;
 }
 
@@ -571,6 +700,7 @@ u64 hash_capacity(u64 n)
 
 bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *err, cudaStream_t s)
 {
+    ix.ch = CompactHash{};
     ix.kind = INDEX_BISECT;
     ix.bucket = nullptr;
     ix.slots = nullptr;

@@ -41,6 +41,7 @@ static int g_test_hold = 0;
 extern int g_solve_variant;
 extern int g_sort_variant;
 extern int g_hash_load_pct;
+extern int g_hash_compact;
 }
 
 static Engine &E() { return Engine::get(); }
@@ -77,6 +78,8 @@ int cgb_get_kernel_stats(cgb_kernel_stats *o)
     o->solve_launches = k.solve_launches;
     o->solve_boards = k.solve_boards;
     o->lookups = k.lookups;
+    o->index_builds = k.index_builds;
+    o->compact_index_builds = k.compact_index_builds;
     return 0;
 }
 
@@ -157,6 +160,12 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         g_dev_mem_cap = (u64)value << 20;
+    } else if (k == "hash_compact") {
+        if (value < 0 || value > 1) {
+            set_error("cgb_set_option: hash_compact must be 0 or 1");
+            return -1;
+        }
+        g_hash_compact = (int)value;
     } else if (k == "fp64_top_layers") {
         if (value < 0 || value > 100000) {
             set_error("cgb_set_option: fp64_top_layers must be in 0..100000");
@@ -189,6 +198,7 @@ long long cgb_get_option(const char *name)
     if (k == "store_chunk_mb") return (long long)(E().store_chunk >> 20);
     if (k == "host_layers_mb") return (long long)(E().host_layers_cap >> 20);
     if (k == "fp64_top_layers") return E().fp64_top_layers;
+    if (k == "hash_compact") return g_hash_compact;
     if (k == "lookback_spin_limit") return g_test_spin;
     if (k == "lookback_hold_first_tile") return g_test_hold;
     if (k == "device_mem_cap_mb") return (long long)(g_dev_mem_cap >> 20);

@@ -59,7 +59,9 @@ long long cgb_get_option(const char *name);
 /* ---- device primitives of one layer step --------------------------------
  * Move + prune + canonicalise every board (the move workers,
  * src/generate.c:133-175; OpenCL move_kernel, src/cl/generate.cl:249-282).
- * d_out needs cap >= 4n slots; *n_out = boards written (unsorted). */
+ * d_out needs cap >= 4n slots; *n_out = boards written (unsorted).  Every
+ * distinct result appears at least once; repeats among the results of the same
+ * block of 1024 consecutive inputs are written once. */
 int cgb_expand_moves(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t cap, uint64_t *n_out);
 /* Total number of empty cells (= size of each spawn stream). */
 int cgb_count_spawns(const uint64_t *d_in, uint64_t n, uint64_t *total);
@@ -130,6 +132,7 @@ typedef struct {
     double hist_ms, onesweep_ms, unique_ms, merge_ms, expand_ms, spawn_ms, solve_ms, index_ms;
     uint64_t hist_bytes, onesweep_bytes, unique_bytes, merge_bytes, expand_bytes, spawn_bytes, solve_bytes;
     uint64_t onesweep_launches, solve_launches, solve_boards, lookups;
+    uint64_t index_builds, compact_index_builds;  /* hash indexes built; of them in 8-byte slots */
 } cgb_kernel_stats;
 int cgb_get_kernel_stats(cgb_kernel_stats *out);
 int cgb_reset_kernel_stats(void);

@@ -95,6 +95,29 @@ def test_tablebase_fp32_fp64_window(cuda, top):
                 assert np.abs(t64[s][1] - t32[s][1].astype(np.float64)).max() <= 1e-6, s
 
 
+def test_fp32_compact_index_matches_wide(cuda):
+    """FP32 tables looked up through 8-byte slots equal those through 16-byte slots, bit for
+    bit (both indexes are exact), and the large layers of LL do take the 8-byte form."""
+    w = configs.get("ll_pruned", end_gen=230)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    old = cuda.get_option("hash_compact")
+    try:
+        cuda.set_option("hash_compact", 0)
+        _, wide, _ = cuda.tablebase(f.initial, f.start, f.end_gen, f.start, f.winstates, precision=32,
+                                    keep_tables=True)
+        cuda.set_option("hash_compact", 1)
+        cuda.reset_kernel_stats()
+        _, comp, _ = cuda.tablebase(f.initial, f.start, f.end_gen, f.start, f.winstates, precision=32,
+                                    keep_tables=True)
+        k = cuda.kernel_stats()
+    finally:
+        cuda.set_option("hash_compact", old)
+    assert k["compact_index_builds"] > 0, k
+    for s in wide:
+        assert np.array_equal(wide[s][1], comp[s][1]), s
+
+
 @pytest.mark.parametrize("host_layers_mb", [65536, 0])
 def test_tablebase_async_copies_match(cuda, host_layers_mb):
     """Layers and tables copied out asynchronously equal the engine's own (LL, pruned, 40 layers),
