@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-formation batched sweep block")
+    ap.add_argument("--no-large", action="store_true", help="skip the large-table (config 5 prefix) block")
+    ap.add_argument("--large-end", type=int, default=70, help="end tile sum of the large-table block")
     ap.add_argument("--cpu-end", type=int, default=None, help="end tile sum of the CPU sample")
     ap.add_argument("--case", default=None, choices=["sort", "expand", "solve"],
                     help="one small kernel case for a profiler capture instead of the benchmark")
@@ -459,6 +461,26 @@ def run_ours(args):
         for v in precision.values():
             v["within_1e-6"] = v["max_abs_err"] <= 1e-6
 
+    # ---- large single table (config 5: LL, free formation, nox 10, prune 64/6/6) up to the
+    # end the reference's digests pin: FP64, layers sliced at max_sort_keys, resident-layer
+    # store with its spill policy.  Kernel share = the kernels' CUDA-event time / the sweep's
+    large = None
+    if not args.no_large and rank == 0:
+        lw = configs.get("ll_large", end_gen=args.large_end)
+        lf = lw.formations[0]
+        device.set_rules(lw.settings)
+        _, _, sl = device.tablebase(lf.initial, lf.start, lf.end_gen, lf.start, lf.winstates, 64)
+        kern = sl["expand_ms"] + sl["sort_ms"] + sl["unique_ms"] + sl["merge_ms"] + sl["solve_kernel_ms"] + \
+            sl["index_ms"]
+        bl = sl["boards_generated"] + sl["boards_solved"]
+        large = {"workload": "ll_large", "end_gen": lf.end_gen, "solve": "fp64", "layers": sl["layers"],
+                 "boards": bl, "total_ms": sl["total_ms"], "gen_ms": sl["gen_ms"], "solve_ms": sl["solve_ms"],
+                 "kernel_ms": kern, "kernel_share": kern / sl["total_ms"] if sl["total_ms"] else None,
+                 "boards_per_s": bl / (sl["total_ms"] / 1000.0) if sl["total_ms"] else None,
+                 "layer_slices": sl["layer_slices"], "spilled_chunks": sl["spilled_chunks"],
+                 "restored_chunks": sl["restored_chunks"]}
+        device.set_rules(wl.settings)
+
     # ---- like for like with the reference arm: the same sample (generate + solve over
     # the reference arm's tile sums) through the drop-in C API, every file written
     like = None
@@ -567,7 +589,8 @@ def run_ours(args):
                 "config": bench_config(args.workload, args.end),
                 "parallelism": f"replicas x{world}", "boards_per_step": boards // max(args.steps, 1),
                 "wall_s": wall, "gpu_launches": gpu_launches, "clocks": clock_summary, "roofline": roofline,
-                "fp32": fp32, "precision": precision, "e2e": e2e, "like_for_like": like, "batch": batch,
+                "fp32": fp32, "precision": precision, "e2e": e2e, "like_for_like": like, "large": large,
+                "batch": batch,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if dist is not None:

@@ -170,6 +170,27 @@ def cli_commands():
     return cmds
 
 
+# play and train draw spawns from rand() seeded with time(NULL) (frontends/cli/main.c:354-475);
+# with time() fixed by a preloaded library both CLIs replay the same game.  train reads
+# its moves from standard input.
+CLI_GAMES = [("play", "0x12000000ffffffff", ""), ("train", "0x12000000ffffffff", "asdwdsaw" * 40)]
+
+
+def fixed_time_lib(outdir):
+    """Builds tests/host/fixed_time.c into outdir/fixed_time.so (gcc) and returns its path."""
+    out = os.path.join(outdir, "fixed_time.so")
+    src = os.path.join(HERE, "..", "host", "fixed_time.c")
+    subprocess.run(["gcc", "-shared", "-fPIC", "-O2", "-o", out, src], check=True)
+    return out
+
+
+def run_game(cli, conf, work, env, cmd, board, stdin, preload):
+    env = dict(env, LD_PRELOAD=preload)
+    r = subprocess.run([cli, f"-C={conf}", cmd, board], cwd=work, env=env, input=stdin, capture_output=True,
+                       text=True, timeout=300)
+    return r.stdout
+
+
 def cmd_cli(args):
     work = tempfile.mkdtemp(prefix="golden_cli_")
     conf = cli_prepare(work)
@@ -182,8 +203,13 @@ def cmd_cli(args):
         out = subprocess.run([REF_CLI, f"-C={conf}"] + c, cwd=work, env=env, capture_output=True, text=True).stdout
         with open(os.path.join(store, f"{i:02d}_{c[0]}.txt"), "w") as f:
             f.write(out)
+    preload = fixed_time_lib(work)
+    for cmd, board, stdin in CLI_GAMES:
+        out = run_game(REF_CLI, conf, work, env, cmd, board, stdin, preload)
+        with open(os.path.join(store, f"game_{cmd}.txt"), "w") as f:
+            f.write(out)
     shutil.rmtree(work)
-    print("cli transcripts:", len(cli_commands()))
+    print("cli transcripts:", len(cli_commands()), "games:", len(CLI_GAMES))
 
 
 # ---------------------------------------------------------------- unit vectors

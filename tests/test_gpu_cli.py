@@ -10,7 +10,7 @@ import pytest
 from helpers import GOLDEN, ROOT, digests
 
 sys.path.insert(0, os.path.join(GOLDEN))
-from make_golden import CLI_WORKLOAD, cli_commands, cli_prepare, sha  # noqa: E402
+from make_golden import CLI_GAMES, CLI_WORKLOAD, cli_commands, cli_prepare, fixed_time_lib, run_game, sha  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
@@ -45,6 +45,18 @@ def test_cli_transcripts(cli_dir, i):
     out = subprocess.run([CLI, f"-C={conf}"] + cmd, cwd=work, env=env, capture_output=True, text=True,
                          timeout=120).stdout
     with open(os.path.join(GOLDEN, "cli", f"{i:02d}_{cmd[0]}.txt")) as f:
+        want = f.read()
+    assert out == want
+
+
+@pytest.mark.parametrize("game", CLI_GAMES, ids=[g[0] for g in CLI_GAMES])
+def test_cli_play_and_train_transcripts(cli_dir, tmp_path, game):
+    """play and train (frontends/cli/main.c:354-475) over this library's tables: with time()
+    fixed (so srand seeds the same spawns) the transcript equals the reference CLI's."""
+    work, conf, env = cli_dir
+    cmd, board, stdin = game
+    out = run_game(CLI, conf, work, env, cmd, board, stdin, fixed_time_lib(str(tmp_path)))
+    with open(os.path.join(GOLDEN, "cli", f"game_{cmd}.txt")) as f:
         want = f.read()
     assert out == want
 
