@@ -123,6 +123,30 @@ __device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
     return true;  // unreachable: the set is never more than half full
 }
 
+// the four moves of b, pruned, canonicalised (over the plan's images when
+// PLANNED, chosen once per warp so that the choice is a uniform branch) and
+// checked against the CTA's set; returns the mask of results to write
+template <bool PLANNED>
+__device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const PruneParams &pp, const CanonPlan &plan,
+                                           unsigned long long *set, u64 r[4])
+{
+    u64 v[4];
+    views(b, v);
+    // a move that merges nothing keeps the multiset of tiles, so it keeps
+    // the input's (passing) prune verdict; merges show as new empty cells
+    const int empties = pp.enabled ? popc64(empty_mask(b)) : 0;
+    u32 mask = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        u64 m;
+        if (move_left(t, v[k], &m) == 2 && !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
+            r[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+            if (set_insert(set, r[k])) mask |= 1u << k;
+        }
+    }
+    return mask;
+}
+
 __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
@@ -142,26 +166,15 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
         const u64 idx = first + threadIdx.x;
         u64 r[4] = {0, 0, 0, 0};
         u32 mask = 0;
+        const u64 b = idx < n ? in[idx] : 0;
+        // the images that can be canonical: the plan's when every board of the warp has its mask
+        const bool planned = __all_sync(0xffffffffu, idx >= n || fixed_pattern(b) == plan.mask);
         if (idx < n) {
-            const u64 b = in[idx];
             // boards of a formation that has reached its last layer stop here
             const bool live = !ff.fid || __ldg(ff.active + __ldg(ff.fid + fixed_pattern(b)));
             if (live && !(pp.enabled && prune_board(b, pp))) {
-                u64 v[4];
-                views(b, v);
-                // a move that merges nothing keeps the multiset of tiles, so it keeps
-                // the input's (passing) prune verdict; merges show as new empty cells
-                const int empties = pp.enabled ? popc64(empty_mask(b)) : 0;
-                const bool planned = fixed_pattern(b) == plan.mask;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    u64 m;
-                    if (move_left(t, v[k], &m) == 2 &&
-                        !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
-                        r[k] = canon_cand(m, planned ? plan.view[k] : 0xFFu);
-                        if (set_insert(set, r[k])) mask |= 1u << k;
-                    }
-                }
+                if (planned) mask = board_moves<true>(t, b, pp, plan, set, r);
+                else mask = board_moves<false>(t, b, pp, plan, set, r);
             }
         }
         const u32 cnt = __popc(mask);
@@ -191,6 +204,20 @@ __global__ void __launch_bounds__(256) count_spawns_kernel(const u64 *__restrict
     if (threadIdx.x == 0 && tot) atomicAdd((unsigned long long *)total, (unsigned long long)tot);
 }
 
+// the canonical 2- and 4-spawn of one cell from the board's images: the
+// maximum over the images in cand (all eight unless PLANNED)
+template <bool PLANNED>
+__device__ __forceinline__ void spawn_max(const u64 im[8], int cell, u32 cand, u64 *m2, u64 *m4)
+{
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        if (PLANNED && !((cand >> k) & 1u)) continue;
+        const int sh = 60 - 4 * image_cell(k, cell);
+        *m2 = umax64(*m2, im[k] | (1ull << sh));
+        *m4 = umax64(*m4, im[k] | (2ull << sh));
+    }
+}
+
 __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restrict__ in, u64 n,
                                                             u64 *__restrict__ out2, u64 *__restrict__ out4,
                                                             u64 cap, u64 *out_count, u32 *err, CanonPlan plan)
@@ -202,6 +229,7 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
         const u64 idx = first + threadIdx.x;
         const u64 b = idx < n ? in[idx] : ~0ull;
         u64 e = idx < n ? empty_mask(b) : 0;
+        const bool planned = __all_sync(0xffffffffu, idx >= n || fixed_pattern(b) == plan.mask);
         const u32 cnt = popc64(e);
         u32 total;
         const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
@@ -216,19 +244,13 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
             // maximum when b has the plan's mask
             u64 im[8];
             images(b, im);
-            const u32 cand = fixed_pattern(b) == plan.mask ? plan.view[0] : 0xFFu;
             while (e) {
                 const int bit = 63 - __clzll(e);  // nibble's low bit
                 e &= ~(1ull << bit);
                 const int cell = (60 - bit) >> 2;
                 u64 m2 = 0, m4 = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    if (!((cand >> k) & 1u)) continue;
-                    const int sh = 60 - 4 * image_cell(k, cell);
-                    m2 = umax64(m2, im[k] | (1ull << sh));
-                    m4 = umax64(m4, im[k] | (2ull << sh));
-                }
+                if (planned) spawn_max<true>(im, cell, plan.view[0], &m2, &m4);
+                else spawn_max<false>(im, cell, 0xFFu, &m2, &m4);
                 out2[pos] = m2;
                 out4[pos] = m4;
                 pos++;

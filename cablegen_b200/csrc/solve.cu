@@ -83,13 +83,14 @@ __device__ __forceinline__ V sorted_lookup(const DevTable<V> &t, u64 key)
     return __ldg(t.keys + lo) == key ? __ldg(t.vals + lo) : V(0);
 }
 
-// continue a linear probe after the first slot missed
+// continue a linear probe after the first slot missed (plain arguments: a
+// reference to the kernel's table would force a copy of it to local memory)
 template <typename V>
-__device__ __noinline__ V hash_probe_rest(const DevTable<V> &t, u64 key, u64 s)
+__device__ __noinline__ V hash_probe_rest(const ulonglong2 *slots, u64 cap, u64 key, u64 s)
 {
-    for (u64 i = 1; i < t.cap; i++) {
-        s = (s + 1 == t.cap) ? 0 : s + 1;
-        const ulonglong2 e = __ldg(t.slots + s);
+    for (u64 i = 1; i < cap; i++) {
+        s = (s + 1 == cap) ? 0 : s + 1;
+        const ulonglong2 e = __ldg(slots + s);
         if (e.x == key) return from_bits<V>(e.y);
         if (e.x == 0) return V(0);
     }
@@ -98,12 +99,11 @@ __device__ __noinline__ V hash_probe_rest(const DevTable<V> &t, u64 key, u64 s)
 
 // continue a compact probe after the home slot held another key
 template <typename V>
-__device__ __noinline__ V compact_probe_rest(const DevTable<V> &t, u64 home, u32 tag0)
+__device__ __noinline__ V compact_probe_rest(const u64 *slots, u64 cap, int dbits, u64 home, u32 tag0)
 {
-    const u64 *w = (const u64 *)t.slots;
-    const u32 last = (1u << t.ch.dbits) - 1u;  // probe distances stay below it (the build checks)
+    const u32 last = (1u << dbits) - 1u;  // probe distances stay below it (the build checks)
     for (u32 d = 1; d + 1 < last; d++) {
-        const u64 e = __ldg(w + ((home + d) & (t.cap - 1)));
+        const u64 e = __ldg(slots + ((home + d) & (cap - 1)));
         if ((u32)e == tag0 + d) return from_bits<V>(e >> 32);
         if ((u32)e == 0u) return V(0);
     }
@@ -123,7 +123,7 @@ __device__ __forceinline__ V table_value(const DevTable<V> &t, u64 key)
         const u64 e = __ldg((const u64 *)t.slots + h);
         if ((u32)e == tag0) return from_bits<V>(e >> 32);
         if ((u32)e == 0u) return V(0);
-        return compact_probe_rest(t, h, tag0);
+        return compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, h, tag0);
     }
     if (t.kind == INDEX_HASH) {
         if (t.cap == 0) return V(0);
@@ -131,7 +131,7 @@ __device__ __forceinline__ V table_value(const DevTable<V> &t, u64 key)
         const ulonglong2 e = __ldg(t.slots + s);
         if (e.x == key) return from_bits<V>(e.y);
         if (e.x == 0) return V(0);
-        return hash_probe_rest(t, key, s);
+        return hash_probe_rest<V>(t.slots, t.cap, key, s);
     }
     return sorted_lookup(t, key);
 }
@@ -199,6 +199,122 @@ struct SpawnSums {
     }
 };
 
+// Direct variant: one thread per board, no queue.  The eight successors of
+// one cell (2 spawns x 4 moves) are formed from the board's four views (the
+// spawned nibble is OR-ed into each view), canonicalised and probed together,
+// so a thread keeps up to eight independent loads in flight.
+constexpr int DIRECT_THREADS = 1024;
+
+template <typename V>
+__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out)
+{
+    if (t.kind == INDEX_HASH && t.ch.on) {
+        u64 h[4], e[4];
+        u32 tag[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && (key[j] & t.ch.cmask) == t.ch.cval;
+            h[j] = compact_home(t.ch, key[j], &tag[j]);
+            e[j] = on ? __ldg((const u64 *)t.slots + h[j]) : 0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if ((u32)e[j] == tag[j]) out[j] = from_bits<V>(e[j] >> 32);
+            else if ((u32)e[j] == 0u) out[j] = V(0);
+            else out[j] = compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, h[j], tag[j]);
+        }
+        return;
+    }
+    if (t.kind == INDEX_HASH) {
+        u64 s[4];
+        ulonglong2 e[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && t.cap;
+            s[j] = on ? home_slot(key[j], t.cap) : 0;
+            e[j] = on ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (!((legal >> j) & 1) || e[j].x == 0) out[j] = V(0);
+            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
+            else out[j] = hash_probe_rest<V>(t.slots, t.cap, key[j], s[j]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) out[j] = ((legal >> j) & 1) ? sorted_lookup(t, key[j]) : V(0);
+    }
+}
+
+// The best values of one empty cell: its eight successors (2 and 4 spawned
+// into each of the board's four views, then the left move), canonicalised --
+// over the plan's images when PLANNED, which the caller picks once per warp so
+// that the image choice is a uniform branch -- and looked up in the s+2 and s+4
+// tables, eight loads in flight.
+template <bool PLANNED, typename V>
+__device__ __forceinline__ void cell_bests(const RowTable &rt, const u64 v[4], int cell, const CanonPlan &plan,
+                                           const DevTable<V> &t2, const DevTable<V> &t4, V &best2, V &best4,
+                                           u32 &probes)
+{
+    u64 k2[4], k4[4];
+    u32 l2 = 0, l4 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int sh = 60 - 4 * view_cell(k, cell);
+        u64 m;
+        if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
+        k2[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+        if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
+        k4[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+    }
+    probes += __popc(l2) + __popc(l4);
+    V p2[4], p4[4];
+    probe4(t2, k2, l2, p2);
+    probe4(t4, k4, l4, p4);
+    best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
+    best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
+}
+
+template <typename V>
+__global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u64 *__restrict__ keys, u64 n,
+                                                                         V *__restrict__ out, DevTable<V> t2,
+                                                                         DevTable<V> t4, SolveRules r,
+                                                                         const unsigned short *g_move,
+                                                                         u64 *probes_out, CanonPlan plan)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    stage_table_s(smem, g_move);
+    const RowTable rt{(const unsigned short *)smem};
+    u32 probes = 0;
+    for (u64 i = (u64)blockIdx.x * DIRECT_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * DIRECT_THREADS) {
+        const u64 b = keys[i];
+        // the images that can be canonical: the plan's when every board of the warp has its mask
+        const bool planned = __all_sync(__activemask(), fixed_pattern(b) == plan.mask);
+        V res;
+        if (satisfied(b, r)) {
+            res = V(1);
+        } else {
+            u64 e = empty_mask(b);
+            const int spaces = popc64(e);
+            u64 v[4];
+            views(b, v);
+            SpawnSums<V> sums;
+            while (e) {  // cells in order 0..15 = highest nibble first
+                const int bit = 63 - __clzll(e);
+                e &= ~(1ull << bit);
+                const int cell = (60 - bit) >> 2;
+                V best2, best4;
+                if (planned) cell_bests<true>(rt, v, cell, plan, t2, t4, best2, best4, probes);
+                else cell_bests<false>(rt, v, cell, plan, t2, t4, best2, best4, probes);
+                sums.add(best2, best4);
+            }
+            res = sums.result(spaces, b, r);
+        }
+        out[i] = res;
+    }
+    add_probes(probes, probes_out);
+}
+
 // Item form: the work of a warp is its boards' (board, empty cell) pairs, not
 // its boards.  Boards have 0..16 empty cells, so one thread per board leaves a
 // warp waiting on its fullest board; here the 32 lanes take the pairs of 32
@@ -212,9 +328,6 @@ constexpr int ITEM_WARPS = ITEM_THREADS / 32;
 constexpr int ITEM_MAX = 32 * 16;  // pairs of 32 boards at most
 template <typename V>
 constexpr int item_smem() { return TABLE_BYTES_S + ITEM_WARPS * (ITEM_MAX * 2 + 2 * 32 * (int)sizeof(V)); }
-
-template <typename V>
-__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out);
 
 template <typename V>
 __global__ void __launch_bounds__(ITEM_THREADS, 1)
@@ -245,7 +358,8 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
             e &= ~(1ull << bit);
             items[j] = (unsigned short)((lane << 4) | ((60 - bit) >> 2));
         }
-        const bool planned = fixed_pattern(b) == plan.mask;
+        // the images that can be canonical: the plan's when every board of the batch has its mask
+        const bool planned = __all_sync(0xffffffffu, !active || fixed_pattern(b) == plan.mask);
         __syncwarp();
         SpawnSums<V> sums;
         for (u32 r0 = 0; r0 < total; r0 += 32) {
@@ -254,29 +368,12 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
             const u32 it = has ? items[j] : 0u;
             const int owner = (int)(it >> 4), cell = (int)(it & 15u);
             const u64 ob = __shfl_sync(0xffffffffu, b, owner);
-            const bool opl = __shfl_sync(0xffffffffu, planned, owner);
             V best2 = 0, best4 = 0;
             if (has) {
                 u64 v[4];
                 views(ob, v);
-                u64 k2[4], k4[4];
-                u32 l2 = 0, l4 = 0;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int sh = 60 - 4 * view_cell(k, cell);
-                    const u32 cand = opl ? plan.view[k] : 0xFFu;
-                    u64 m;
-                    if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
-                    k2[k] = canon_cand(m, cand);
-                    if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
-                    k4[k] = canon_cand(m, cand);
-                }
-                probes += __popc(l2) + __popc(l4);
-                V p2[4], p4[4];
-                probe4(t2, k2, l2, p2);
-                probe4(t4, k4, l4, p4);
-                best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
-                best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
+                if (planned) cell_bests<true>(rt, v, cell, plan, t2, t4, best2, best4, probes);
+                else cell_bests<false>(rt, v, cell, plan, t2, t4, best2, best4, probes);
             }
             best_sh[lane] = best2;
             best_sh[32 + lane] = best4;
@@ -289,105 +386,6 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
         }
         if (active) out[i] = sat ? V(1) : sums.result(spaces, b, r);
         __syncwarp();
-    }
-    add_probes(probes, probes_out);
-}
-
-// Direct variant: one thread per board, no queue.  The eight successors of
-// one cell (2 spawns x 4 moves) are formed from the board's four views (the
-// spawned nibble is OR-ed into each view), canonicalised and probed together,
-// so a thread keeps up to eight independent loads in flight.
-constexpr int DIRECT_THREADS = 1024;
-
-template <typename V>
-__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out)
-{
-    if (t.kind == INDEX_HASH && t.ch.on) {
-        u64 h[4], e[4];
-        u32 tag[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const bool on = (legal >> j) & 1 && (key[j] & t.ch.cmask) == t.ch.cval;
-            h[j] = compact_home(t.ch, key[j], &tag[j]);
-            e[j] = on ? __ldg((const u64 *)t.slots + h[j]) : 0ull;
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if ((u32)e[j] == tag[j]) out[j] = from_bits<V>(e[j] >> 32);
-            else if ((u32)e[j] == 0u) out[j] = V(0);
-            else out[j] = compact_probe_rest(t, h[j], tag[j]);
-        }
-        return;
-    }
-    if (t.kind == INDEX_HASH) {
-        u64 s[4];
-        ulonglong2 e[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const bool on = (legal >> j) & 1 && t.cap;
-            s[j] = on ? home_slot(key[j], t.cap) : 0;
-            e[j] = on ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            if (!((legal >> j) & 1) || e[j].x == 0) out[j] = V(0);
-            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
-            else out[j] = hash_probe_rest(t, key[j], s[j]);
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) out[j] = ((legal >> j) & 1) ? sorted_lookup(t, key[j]) : V(0);
-    }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u64 *__restrict__ keys, u64 n,
-                                                                         V *__restrict__ out, DevTable<V> t2,
-                                                                         DevTable<V> t4, SolveRules r,
-                                                                         const unsigned short *g_move,
-                                                                         u64 *probes_out, CanonPlan plan)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    stage_table_s(smem, g_move);
-    const RowTable rt{(const unsigned short *)smem};
-    u32 probes = 0;
-    for (u64 i = (u64)blockIdx.x * DIRECT_THREADS + threadIdx.x; i < n; i += (u64)gridDim.x * DIRECT_THREADS) {
-        const u64 b = keys[i];
-        V res;
-        if (satisfied(b, r)) {
-            res = V(1);
-        } else {
-            u64 e = empty_mask(b);
-            const int spaces = popc64(e);
-            u64 v[4];
-            views(b, v);
-            const bool planned = fixed_pattern(b) == plan.mask;
-            SpawnSums<V> sums;
-            while (e) {  // cells in order 0..15 = highest nibble first
-                const int bit = 63 - __clzll(e);
-                e &= ~(1ull << bit);
-                const int cell = (60 - bit) >> 2;
-                u64 k2[4], k4[4];
-                u32 l2 = 0, l4 = 0;
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int sh = 60 - 4 * view_cell(k, cell);
-                    const u32 cand = planned ? plan.view[k] : 0xFFu;
-                    u64 m;
-                    if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
-                    k2[k] = canon_cand(m, cand);
-                    if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
-                    k4[k] = canon_cand(m, cand);
-                }
-                probes += __popc(l2) + __popc(l4);
-                V p2[4], p4[4];
-                probe4(t2, k2, l2, p2);
-                probe4(t4, k4, l4, p4);
-                sums.add(vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3])), vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3])));
-            }
-            res = sums.result(spaces, b, r);
-        }
-        out[i] = res;
     }
     add_probes(probes, probes_out);
 }

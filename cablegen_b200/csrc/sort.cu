@@ -349,18 +349,31 @@ __global__ void __launch_bounds__(SORT_THREADS, 5)
 
 // ---------------------------------------------------------------------------
 // Third form of the ballot pass, for byte digits of the key: the tile's body
-// is specialised for full tiles (no bounds tests on 4095 of every 4096 keys),
+// is specialised for full tiles (no bounds tests on all but the last tile),
 // the ranking phase reads only the 32-bit word that holds the digit, digits
 // come out of words with one byte permute, and each bin keeps one combined
-// offset (global start - local start) for the final write.
-template <bool FULL>
+// offset (global start - local start) for the final write.  THREADS x 16 keys
+// per tile: 256 threads (4096 keys, five CTAs per SM) or 512 (8192 keys, two
+// CTAs per SM, half the per-tile look-back and scans per key).
+template <int THREADS>
+struct BytePassSmem {
+    static constexpr int TILE = THREADS * BAL_KPT;
+    u64 keys[TILE];
+    u32 warp_hist[THREADS / 32][RADIX];
+    u32 bin_local[RADIX];
+    u32 bin_delta[RADIX];
+    u32 scan[33];
+    u32 tile;
+};
+
+template <int THREADS, bool FULL>
 __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
                                                const u32 *__restrict__ digit_hist, u32 *lookback, u32 tile, u32 *err,
-                                               u64 *keys_sh, u32 (*warp_hist)[RADIX], u32 *bin_local, u32 *bin_delta,
-                                               u32 *scan_scratch)
+                                               BytePassSmem<THREADS> &S)
 {
+    constexpr u32 TILE = (u32)BytePassSmem<THREADS>::TILE;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const u32 tile_base = tile * BAL_TILE;
+    const u32 tile_base = tile * TILE;
     const u32 warp_base = tile_base + warp * (BAL_KPT * 32);
     const u32 *src_w = (const u32 *)src + (shift >= 32 ? 1 : 0);   // little-endian words of the keys
     const u32 sel = 0x4440u | (u32)((shift >> 3) & 3);              // the digit's byte, zero above it
@@ -389,14 +402,14 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
             const u32 bj = __ballot_sync(0xffffffffu, (d >> j) & 1);
             peers &= ((d >> j) & 1) ? bj : ~bj;
         }
-        const u32 base = warp_hist[warp][d];   // every peer reads the same word
+        const u32 base = S.warp_hist[warp][d];   // every peer reads the same word
         __syncwarp();
         const bool leader = (peers & lt) == 0;
         if (FULL) {
-            if (leader) warp_hist[warp][d] = base + __popc(peers);
+            if (leader) S.warp_hist[warp][d] = base + __popc(peers);
         } else {
             const u32 idx = warp_base + i * 32 + lane;
-            if (idx < n && leader) warp_hist[warp][d] = base + __popc(peers);
+            if (idx < n && leader) S.warp_hist[warp][d] = base + __popc(peers);
         }
         __syncwarp();
         const u32 r = base + __popc(peers & lt);
@@ -404,19 +417,21 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
         else rank2[i >> 1] = r;
     }
     __syncthreads();
-    const u32 d = threadIdx.x;  // SORT_THREADS == RADIX
+    const u32 d = threadIdx.x;  // threads below RADIX own one bin each
     u32 cnt = 0;
+    if (d < RADIX) {
 #pragma unroll
-    for (int w = 0; w < SORT_THREADS / 32; w++) {
-        const u32 c = warp_hist[w][d];
-        warp_hist[w][d] = cnt;
-        cnt += c;
+        for (int w = 0; w < THREADS / 32; w++) {
+            const u32 c = S.warp_hist[w][d];
+            S.warp_hist[w][d] = cnt;
+            cnt += c;
+        }
+        if (tile != 0 || !g_hold_first_tile)
+            st_relaxed(lookback + (u64)tile * RADIX + d, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
     }
-    u32 *lb = lookback + (u64)tile * RADIX + d;
-    if (tile != 0 || !g_hold_first_tile) st_relaxed(lb, (tile == 0 ? LB_PRE : LB_AGG) | cnt);
     u32 total;
-    const u32 lstart = block_exclusive_scan<u32>(cnt, scan_scratch, &total);
-    bin_local[d] = lstart;
+    const u32 lstart = block_exclusive_scan<u32>(cnt, S.scan, &total);
+    if (d < RADIX) S.bin_local[d] = lstart;
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < BAL_KPT; i++) {
@@ -425,49 +440,44 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
             const u64 key = src[idx];
             const u32 dd = __byte_perm(dg[i / 4], 0, 0x4440u | (u32)(i % 4));
             const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xFFFF;
-            keys_sh[bin_local[dd] + warp_hist[warp][dd] + r] = key;
+            S.keys[S.bin_local[dd] + S.warp_hist[warp][dd] + r] = key;
         }
     }
     u32 excl = 0;
-    if (tile != 0) {
+    if (d < RADIX && tile != 0) {
         excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
-        st_relaxed(lb, LB_PRE | (excl + cnt));
+        st_relaxed(lookback + (u64)tile * RADIX + d, LB_PRE | (excl + cnt));
     }
-    const u32 gexcl = block_exclusive_scan<u32>(digit_hist[d], scan_scratch, &total);
-    bin_delta[d] = gexcl + excl - lstart;
+    const u32 gexcl = block_exclusive_scan<u32>(d < RADIX ? digit_hist[d] : 0u, S.scan, &total);
+    if (d < RADIX) S.bin_delta[d] = gexcl + excl - lstart;
     __syncthreads();
     const bool hiw = shift >= 32;
-    const u32 tile_n = FULL ? (u32)BAL_TILE : min((u32)BAL_TILE, n - tile_base);
+    const u32 tile_n = FULL ? TILE : min(TILE, n - tile_base);
 #pragma unroll 4
-    for (u32 j = threadIdx.x; j < tile_n; j += SORT_THREADS) {
-        const u64 key = keys_sh[j];
+    for (u32 j = threadIdx.x; j < tile_n; j += THREADS) {
+        const u64 key = S.keys[j];
         const u32 dd = __byte_perm(hiw ? (u32)(key >> 32) : (u32)key, 0, sel);
-        const u32 g = bin_delta[dd] + j;
+        const u32 g = S.bin_delta[dd] + j;
         if (g < n) dst[g] = key;
         else atomicOr(err, ERR_CAPACITY);
     }
 }
 
-__global__ void __launch_bounds__(SORT_THREADS, 5)
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == 256 ? 5 : 2)
     onesweep_byte_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
                          const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err)
 {
-    __shared__ u64 keys_sh[BAL_TILE];
-    __shared__ u32 warp_hist[SORT_THREADS / 32][RADIX];
-    __shared__ u32 bin_local[RADIX];
-    __shared__ u32 bin_delta[RADIX];
-    __shared__ u32 scan_scratch[33];
-    __shared__ u32 tile_sh;
-    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
-    for (int i = threadIdx.x; i < (SORT_THREADS / 32) * RADIX; i += SORT_THREADS) (&warp_hist[0][0])[i] = 0;
+    extern __shared__ __align__(16) unsigned char byte_smem[];
+    BytePassSmem<THREADS> &S = *reinterpret_cast<BytePassSmem<THREADS> *>(byte_smem);
+    if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
+    for (int i = threadIdx.x; i < (THREADS / 32) * RADIX; i += THREADS) (&S.warp_hist[0][0])[i] = 0;
     __syncthreads();
-    const u32 tile = tile_sh;
-    if ((u64)(tile + 1) * BAL_TILE <= n)
-        byte_pass_tile<true>(src, dst, n, shift, digit_hist, lookback, tile, err, keys_sh, warp_hist, bin_local,
-                             bin_delta, scan_scratch);
+    const u32 tile = S.tile;
+    if ((u64)(tile + 1) * BytePassSmem<THREADS>::TILE <= n)
+        byte_pass_tile<THREADS, true>(src, dst, n, shift, digit_hist, lookback, tile, err, S);
     else
-        byte_pass_tile<false>(src, dst, n, shift, digit_hist, lookback, tile, err, keys_sh, warp_hist, bin_local,
-                              bin_delta, scan_scratch);
+        byte_pass_tile<THREADS, false>(src, dst, n, shift, digit_hist, lookback, tile, err, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -637,7 +647,22 @@ static int pipe_grid(int device)
     return grid;
 }
 
-int g_sort_variant = 3;  // 0: match ranking, 1: ballot ranking, 2: pipelined persistent, 3: byte-digit ballot
+// 0: match ranking, 1: ballot ranking, 2: pipelined persistent, 3: byte-digit ballot
+// (4096-key tiles), 4: byte-digit ballot with 8192-key tiles
+int g_sort_variant = 3;
+
+// the 8192-key byte pass needs more than the default 48 KiB of shared memory
+static bool byte512_attr()
+{
+    static bool done = false;
+    if (!done) {
+        if (!CGB_CUDA(cudaFuncSetAttribute(onesweep_byte_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sizeof(BytePassSmem<512>))))
+            return false;
+        done = true;
+    }
+    return true;
+}
 
 // test switches of the look-back waits (see g_spin_limit); 0 restores the default limit
 bool set_lookback_test(u32 spin_limit, int hold_first_tile)
@@ -978,7 +1003,11 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         pgrid = pipe_grid(dev);
         if (pgrid <= 0 || (((uintptr_t)keys | (uintptr_t)tmp) & 15)) variant = 1;
     }
-    const u32 pass_tiles = variant == 2 ? ceil_div(n, PIPE_TILE) : (variant == 1 || variant == 3) ? ceil_div(n, BAL_TILE) : tiles;
+    const u32 pass_tiles = variant == 2   ? ceil_div(n, PIPE_TILE)
+                           : variant == 4 ? ceil_div(n, 512 * BAL_KPT)
+                           : (variant == 1 || variant == 3) ? ceil_div(n, BAL_TILE)
+                                                            : tiles;
+    if (variant == 4 && !byte512_attr()) return false;
     u64 *src = keys, *dst = tmp;
     for (int p = 0; p < np; p++) {
         const int d = digits[p];
@@ -993,10 +1022,13 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
                                                                   ws.small + W_HIST + d * RADIX, ws.lookback,
                                                                   ws.small + W_CTR + p, ws.small + W_ERR);
         else if (variant == 3)
-            onesweep_byte_kernel<<<ceil_div(n, BAL_TILE), SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d,
-                                                                                ws.small + W_HIST + d * RADIX,
-                                                                                ws.lookback, ws.small + W_CTR + p,
-                                                                                ws.small + W_ERR);
+            onesweep_byte_kernel<256><<<ceil_div(n, 256 * BAL_KPT), 256, sizeof(BytePassSmem<256>), s>>>(
+                src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX, ws.lookback, ws.small + W_CTR + p,
+                ws.small + W_ERR);
+        else if (variant == 4)
+            onesweep_byte_kernel<512><<<ceil_div(n, 512 * BAL_KPT), 512, sizeof(BytePassSmem<512>), s>>>(
+                src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX, ws.lookback, ws.small + W_CTR + p,
+                ws.small + W_ERR);
         else
             onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
                                                            ws.lookback, ws.small + W_CTR + p, ws.small + W_ERR);

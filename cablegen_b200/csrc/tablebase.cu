@@ -105,9 +105,9 @@ int cgb_set_option(const char *name, long long value)
         }
         g_solve_variant = (int)value;
     } else if (k == "sort_variant") {
-        if (value < 0 || value > 3) {
-            set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking), 2 (pipelined) "
-                      "or 3 (byte-digit ballot ranking)");
+        if (value < 0 || value > 4) {
+            set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking), 2 (pipelined), "
+                      "3 (byte-digit ballot ranking) or 4 (byte-digit, 8192-key tiles)");
             return -1;
         }
         g_sort_variant = (int)value;
