@@ -6,7 +6,8 @@ The knobs (cgb_set_option):
   match, 1 with eight ballots per digit (keys re-read from L2 for the local scatter), 2 keeps
   persistent CTAs that bulk-copy the next tile into shared memory while ranking the current one,
   3 is the ballot pass specialised for byte digits (full tiles without bounds tests, digits read
-  from the one 32-bit word that holds them);
+  from the one 32-bit word that holds them), 4 the same with 8192-key tiles of 512 threads (the
+  tile-size knob);
 * ``solve_variant`` -- 0 one thread per board, 1 the (board, empty cell) pairs of 32 boards
   spread over a warp;
 * ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
@@ -30,7 +31,7 @@ from typing import Dict, Optional
 from . import configs, device
 
 KNOBS = {
-    "sort_variant": [3, 1, 0, 2],
+    "sort_variant": [3, 4, 1, 0, 2],
     "solve_variant": [1, 0],
     "hash_load_pct": [0, 25, 45],
 }

@@ -42,7 +42,7 @@ def test_expand_spawns(cuda):
 SIZES = [0, 1, 2, 31, 4095, 4096, 4097, 8193, 100_000, 1_000_003, 5_000_001]
 
 
-@pytest.fixture(params=[0, 1, 2, 3], ids=["match", "ballot", "pipelined", "byte"])
+@pytest.fixture(params=[0, 1, 2, 3, 4], ids=["match", "ballot", "pipelined", "byte", "byte8k"])
 def sort_variant(cuda, request):
     old = cuda.get_option("sort_variant")
     cuda.set_option("sort_variant", request.param)
