@@ -320,6 +320,18 @@ delete_boards = false
 """)
 
 
+def free_2x4_nox(seed: int = SEED, end_gen: int = 300) -> Workload:
+    """Config 5's rules (free formation: the 0xf cells move like tiles; nox: a board holding
+    the nox tile wins) on the small 2x4 formation, where a 64 tile (nox 6) is reachable, so
+    the nox path yields nonzero probabilities."""
+    w = plain_2x4(seed)
+    w.name = "free_2x4_nox"
+    w.settings = Settings(free_formation=True, ignore_f=False, nox=6)
+    w.formations[0].end_gen = end_gen
+    w.description = f"2x4 formation, free formation, nox 6 (a 64 tile wins), end {end_gen}"
+    return w
+
+
 WORKLOADS = {
     "plain_2x4": plain_2x4,
     "plain_2x4_nearwall": plain_2x4_nearwall,
@@ -328,6 +340,7 @@ WORKLOADS = {
     "dpdf": dpdf,
     "batch64": batch64,
     "ll_large": ll_large,
+    "free_2x4_nox": free_2x4_nox,
 }
 
 

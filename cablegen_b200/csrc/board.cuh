@@ -277,8 +277,9 @@ __device__ __forceinline__ int move_left(const RowTable &t, u64 y, u64 *out)
 // CanonPlan holds them for boards whose fixed_pattern() equals `mask`; a
 // board with any other mask uses all eight (cand 0xff).
 struct CanonPlan {
-    u32 mask = 0xFFFFFFFFu;      // fixed_pattern() the plan is for (never equal: no plan)
-    unsigned char view[4] = {0xFF, 0xFF, 0xFF, 0xFF};  // images for a move result in view k
+    u32 mask = 0xFFFFFFFFu;   // fixed_pattern() the plan is for (never equal: no plan)
+    u32 views = 0xFFFFFFFFu;  // byte k: images for a move result in view k
+    __host__ __device__ __forceinline__ u32 cand(int k) const { return (views >> (8 * k)) & 0xFFu; }
 };
 
 // cand: bit i = image i of images() (id, V, H, VH, T, VT, HT, VHT)
@@ -353,7 +354,7 @@ inline CanonPlan make_canon_plan(u64 b, bool free_formation)
         unsigned char cand = 0;
         for (int i = 0; i < 8; i++)
             if (leading_f(im[i]) == best) cand |= (unsigned char)(1u << i);
-        p.view[k] = best > 0 ? cand : 0xFF;
+        p.views = (p.views & ~(0xFFu << (8 * k))) | ((u32)(best > 0 ? cand : 0xFF) << (8 * k));
     }
     p.mask = fixed_pattern(b);
     return p;

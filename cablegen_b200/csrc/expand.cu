@@ -140,7 +140,7 @@ __device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const Prune
     for (int k = 0; k < 4; k++) {
         u64 m;
         if (move_left(t, v[k], &m) == 2 && !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
-            r[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+            r[k] = PLANNED ? canon_cand(m, plan.cand(k)) : canonical(m);
             if (set_insert(set, r[k])) mask |= 1u << k;
         }
     }
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256) expand_spawns_kernel(const u64 *__restric
                 e &= ~(1ull << bit);
                 const int cell = (60 - bit) >> 2;
                 u64 m2 = 0, m4 = 0;
-                if (planned) spawn_max<true>(im, cell, plan.view[0], &m2, &m4);
+                if (planned) spawn_max<true>(im, cell, plan.cand(0), &m2, &m4);
                 else spawn_max<false>(im, cell, 0xFFu, &m2, &m4);
                 out2[pos] = m2;
                 out4[pos] = m4;

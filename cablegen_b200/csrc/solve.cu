@@ -263,9 +263,9 @@ __device__ __forceinline__ void cell_bests(const RowTable &rt, const u64 v[4], i
         const int sh = 60 - 4 * view_cell(k, cell);
         u64 m;
         if (move_left(rt, v[k] | (1ull << sh), &m) == 2) l2 |= 1u << k;
-        k2[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+        k2[k] = PLANNED ? canon_cand(m, plan.cand(k)) : canonical(m);
         if (move_left(rt, v[k] | (2ull << sh), &m) == 2) l4 |= 1u << k;
-        k4[k] = PLANNED ? canon_cand(m, plan.view[k]) : canonical(m);
+        k4[k] = PLANNED ? canon_cand(m, plan.cand(k)) : canonical(m);
     }
     probes += __popc(l2) + __popc(l4);
     V p2[4], p4[4];
@@ -273,6 +273,63 @@ __device__ __forceinline__ void cell_bests(const RowTable &rt, const u64 v[4], i
     probe4(t4, k4, l4, p4);
     best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
     best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
+}
+
+// One probe of a table (the successor is looked up only when its move was legal).
+template <typename V>
+__device__ __forceinline__ V probe1(const DevTable<V> &t, u64 key, bool legal)
+{
+    if (!legal) return V(0);
+    if (t.kind == INDEX_HASH && t.ch.on) {
+        if ((key & t.ch.cmask) != t.ch.cval) return V(0);
+        u32 tag0;
+        const u64 h = compact_home(t.ch, key, &tag0);
+        const u64 e = __ldg((const u64 *)t.slots + h);
+        if ((u32)e == tag0) return from_bits<V>(e >> 32);
+        if ((u32)e == 0u) return V(0);
+        return compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, h, tag0);
+    }
+    if (t.kind == INDEX_HASH) {
+        if (t.cap == 0) return V(0);
+        const u64 s = home_slot(key, t.cap);
+        const ulonglong2 e = __ldg(t.slots + s);
+        if (e.x == key) return from_bits<V>(e.y);
+        if (e.x == 0) return V(0);
+        return hash_probe_rest<V>(t.slots, t.cap, key, s);
+    }
+    return sorted_lookup(t, key);
+}
+
+// cell_bests with the four views in a loop that is not unrolled: one view's
+// two successors per iteration (two loads in flight per lane, hidden by the
+// other warps), a quarter of the code.  The unrolled body of all eight
+// successors is large enough that warps wait on instruction fetch.
+template <bool PLANNED, typename V>
+__device__ __forceinline__ void cell_bests_rolled(const RowTable &rt, u64 b, int cell, const CanonPlan &plan,
+                                                  const DevTable<V> &t2, const DevTable<V> &t4, V &best2, V &best4,
+                                                  u32 &probes)
+{
+    const Half h = halves(b), t = transpose(h);
+    const int r0 = cell >> 2, q0 = cell & 3;
+    best2 = V(0);
+    best4 = V(0);
+#pragma unroll 1
+    for (int k = 0; k < 4; k++) {
+        // view k: id, H, T, H.T; the cell of the spawn in it
+        const Half x = (k & 2) ? t : h;
+        const u64 y = (k & 1) ? whole(flip_h(x)) : whole(x);
+        const int row = (k & 2) ? q0 : r0;
+        const int col = ((k & 2) ? r0 : q0) ^ ((k & 1) ? 3 : 0);
+        const int sh = 60 - 4 * (4 * row + col);
+        u64 m2, m4;
+        const bool ok2 = move_left(rt, y | (1ull << sh), &m2) == 2;
+        const bool ok4 = move_left(rt, y | (2ull << sh), &m4) == 2;
+        const u64 c2 = PLANNED ? canon_cand(m2, plan.cand(k)) : canonical(m2);
+        const u64 c4 = PLANNED ? canon_cand(m4, plan.cand(k)) : canonical(m4);
+        probes += (u32)ok2 + (u32)ok4;
+        best2 = vmax(best2, probe1(t2, c2, ok2));
+        best4 = vmax(best4, probe1(t4, c4, ok4));
+    }
 }
 
 template <typename V>
@@ -370,10 +427,8 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
             const u64 ob = __shfl_sync(0xffffffffu, b, owner);
             V best2 = 0, best4 = 0;
             if (has) {
-                u64 v[4];
-                views(ob, v);
-                if (planned) cell_bests<true>(rt, v, cell, plan, t2, t4, best2, best4, probes);
-                else cell_bests<false>(rt, v, cell, plan, t2, t4, best2, best4, probes);
+                if (planned) cell_bests_rolled<true>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
+                else cell_bests_rolled<false>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
             }
             best_sh[lane] = best2;
             best_sh[32 + lane] = best4;

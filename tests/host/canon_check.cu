@@ -46,12 +46,12 @@ int main(int argc, char **argv)
                 views(x, v);
                 for (int k = 0; k < 4; k++) {
                     checked++;
-                    if (canon_cand(v[k], plan.view[k]) != canonical(v[k])) bad++;
+                    if (canon_cand(v[k], plan.cand(k)) != canonical(v[k])) bad++;
                 }
             }
         }
         std::printf("%04x %llu %llu", cells, (unsigned long long)checked, (unsigned long long)bad);
-        for (int k = 0; k < 4; k++) std::printf(" %d", __builtin_popcount(plan0.view[k]));
+        for (int k = 0; k < 4; k++) std::printf(" %d", __builtin_popcount(plan0.cand(k)));
         std::printf("\n");
     }
     return 0;

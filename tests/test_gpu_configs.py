@@ -41,3 +41,7 @@ def test_dpdf_full_bit_exact(cuda):
 def test_ll_large_prefix_bit_exact(cuda):
     st = _check(cuda, "ll_large", "ll_large_end70")
     assert st["layers"] == 28
+
+
+def test_free_formation_nox_bit_exact(cuda):
+    _check(cuda, "free_2x4_nox", "free_2x4_nox")
