@@ -146,7 +146,8 @@ struct Engine {
     HostArena host_layers;      // host copies of a sweep's layers (layers and tables both wanted)
     u64 host_layers_cap = 64ull << 30;  // bytes; beyond it tables carry their own key copy
     bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
-    bool spawn_layer(GenTimes *tm);
+    bool spawn_layer(GenTimes *tm, bool unique_streams = false);
+    bool sort_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, DevBuf<u64> **out, GenTimes *tm);
     bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm);
     bool merge_into(DevBuf<u64> &acc, const u64 *run, u64 n);
     // layers start..end from the input set of layer `start`; h_carry = the

@@ -95,7 +95,7 @@ bool spawn_from(DevBuf<u64> &in, DevBuf<u64> *n2, DevBuf<u64> *n4)
     if (!E().ready) return false;
     std::swap(E().gen.moved, in);
     drop(in, E().stream);  // the engine's previous layer buffer
-    if (!E().spawn_layer(nullptr)) return false;
+    if (!E().spawn_layer(nullptr, true)) return false;  // the seam's contract: unique streams
     std::swap(*n2, E().gen.u2);
     std::swap(*n4, E().gen.u4_next);
     note_vram();

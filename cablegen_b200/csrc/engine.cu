@@ -369,7 +369,22 @@ bool Engine::sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, De
     return true;
 }
 
-// acc = acc u run (both sorted unique), through the scratch buffer t
+// sort of n raw keys in x (y = scratch), repeats kept: the merge that takes the
+// result drops them; returns the buffer holding the sorted keys
+bool Engine::sort_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, DevBuf<u64> **out, GenTimes *tm)
+{
+    u64 *sorted = x.p;
+    SortStats st;
+    if (!sort_keys(x.p, y.p, n, &sorted, ws, stream, &st)) return false;
+    if (tm) {
+        tm->sorted_keys += n;
+        tm->sort_passes += (u64)st.passes * n;
+    }
+    *out = (sorted == x.p) ? &x : &y;
+    return true;
+}
+
+// acc = acc u run (both sorted), through the scratch buffer t
 bool Engine::merge_into(DevBuf<u64> &acc, const u64 *run, u64 n)
 {
     cudaStream_t s = stream;
@@ -411,10 +426,11 @@ bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
     return true;
 }
 
-// U2 / U4: sorted unique canonical 2-spawns and 4-spawns of the moved layer;
+// U2 / U4: sorted canonical 2-spawns and 4-spawns of the moved layer (unique
+// when unique_streams; else repeats stay for the next merge to drop);
 // U2 lands in g.u2, U4 in g.u4_next.  Spawn streams longer than max_sort_keys
 // are produced slice by slice and merged.
-bool Engine::spawn_layer(GenTimes *tm)
+bool Engine::spawn_layer(GenTimes *tm, bool unique_streams)
 {
     cudaStream_t s = stream;
     GenBuffers &g = gen;
@@ -446,12 +462,21 @@ bool Engine::spawn_layer(GenTimes *tm)
         u64 ns = 0;
         if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s, plan)) return false;
         // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort
-        // c[1] with the buffer the first sort left free
+        // c[1] with the buffer the first sort left free.  Without unique_streams
+        // the sorted streams keep their repeats: every later merge drops them
         DevBuf<u64> *u2 = nullptr, *u4 = nullptr;
-        u64 n2 = 0, n4 = 0;
-        if (!sort_unique_step(g.c[0], g.c[2], ns, &n2, &u2, tm)) return false;
+        u64 n2 = ns, n4 = ns;
+        if (unique_streams) {
+            if (!sort_unique_step(g.c[0], g.c[2], ns, &n2, &u2, tm)) return false;
+        } else if (!sort_step(g.c[0], g.c[2], ns, &u2, tm)) {
+            return false;
+        }
         DevBuf<u64> &spare = (u2 == &g.c[0]) ? g.c[2] : g.c[0];
-        if (!sort_unique_step(g.c[1], spare, ns, &n4, &u4, tm)) return false;
+        if (unique_streams) {
+            if (!sort_unique_step(g.c[1], spare, ns, &n4, &u4, tm)) return false;
+        } else if (!sort_step(g.c[1], spare, ns, &u4, tm)) {
+            return false;
+        }
         if (!chunked) {
             std::swap(g.u2, *u2);
             g.u2.n = n2;

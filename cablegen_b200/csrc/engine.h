@@ -34,7 +34,8 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
 bool sort_check(SortWorkspace &ws, cudaStream_t s);
 // out must not alias in
 bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s);
-// sorted union of two sorted duplicate-free runs, without repeats
+// sorted union of two sorted runs, without repeats (repeats inside a run are
+// dropped as well)
 bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_out, SortWorkspace &ws,
                   cudaStream_t s);
 

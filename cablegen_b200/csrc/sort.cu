@@ -12,8 +12,9 @@
 //   boards share) are skipped.
 // * unique: adjacent-difference flags, ballot/popc compaction, decoupled
 //   look-back for the tile prefix.
-// * merge_unique: merge-path partition of two sorted unique runs, per-thread
-//   sequential merge in shared memory, the same compaction.
+// * merge_unique: merge-path partition of two sorted runs, per-thread
+//   sequential merge in shared memory, the same compaction (repeats inside a
+//   run are dropped like repeats across the runs).
 //
 // Every look-back wait is bounded (SPIN_LIMIT polls); on timeout the kernel
 // sets ERR_LOOKBACK_TIMEOUT in the error word and finishes without waiting.
@@ -981,7 +982,9 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         return false;
     }
     if (!ws.reserve(((n + SORT_TILE - 1) / SORT_TILE + 1) * RADIX, s)) return false;
-    if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (W_COUNT + 1) * sizeof(u32), s))) return false;
+    // histograms and tile counters start at zero; the error word keeps what an
+    // earlier sort left for the next unique or merge to report
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small, 0, (ws.err_dirty ? W_ERR : W_COUNT + 1) * sizeof(u32), s))) return false;
     const int hist_blocks = (int)std::min<u64>((n + 255) / 256, (u64)NUM_SMS_B200 * 8);
     kclock().begin(s, &kstats().hist_ms);
     digit_histogram_kernel<<<hist_blocks, 256, 0, s>>>(keys, n, ws.small + W_HIST);
@@ -1098,7 +1101,15 @@ bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_o
     // 64-bit look-back words, then the splits (both fit in the u32 look-back area)
     u64 *lb = (u64 *)ws.lookback;
     u64 *splits = lb + ((u64)tiles + 1);
-    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT64 + 2 - W_CTR) * sizeof(u32), s))) return false;
+    // tile counters and counts start at zero; the error word too, unless sorts
+    // before this merge left errors in it (reported below with the merge's own)
+    if (ws.err_dirty) {
+        if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_ERR - W_CTR) * sizeof(u32), s)) ||
+            !CGB_CUDA(cudaMemsetAsync(ws.small + W_COUNT, 0, (W_COUNT64 + 2 - W_COUNT) * sizeof(u32), s)))
+            return false;
+    } else if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_COUNT64 + 2 - W_CTR) * sizeof(u32), s))) {
+        return false;
+    }
     ws.err_dirty = false;
     if (!CGB_CUDA(cudaMemsetAsync(lb, 0, ((u64)tiles + 1) * sizeof(u64), s))) return false;
     kclock().begin(s, &kstats().merge_ms);
