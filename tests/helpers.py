@@ -48,22 +48,27 @@ def sweep_digests(cuda, form, precision=64):
         try:
             h = hashlib.sha256()
             for p in parts:
-                h.update(p)
+                mv = memoryview(p).cast("B")
+                for o in range(0, len(mv), 1 << 28):   # 256 MiB at a time
+                    h.update(mv[o:o + (1 << 28)])
             store[key] = h.hexdigest()
         finally:
             gate.release()
 
+    def copy(ptr, n):
+        # layers of large workloads exceed 2^31 bytes: copy through numpy, not string_at
+        if not n:
+            return np.zeros(0, np.uint64)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint64)), shape=(n,)).copy()
+
     def on_layer(s, ptr, n):
         gate.acquire()
-        data = C.string_at(ptr, 8 * n) if n else b""
-        futures.append(pool.submit(digest, got_layers, s, [data]))
+        futures.append(pool.submit(digest, got_layers, s, [copy(ptr, n)]))
 
     def on_table(s, kptr, vptr, n, prec):
         assert prec == 64
         gate.acquire()
-        keys = C.string_at(kptr, 8 * n) if n else b""
-        vals = C.string_at(vptr, 8 * n) if n else b""
-        futures.append(pool.submit(digest, got_tables, s, [keys, vals]))
+        futures.append(pool.submit(digest, got_tables, s, [copy(kptr, n), copy(vptr, n)]))
 
     _, _, st = cuda.tablebase(form.initial, form.start, form.end_gen, form.start, form.winstates,
                               precision=precision, layer_fn=on_layer, table_fn=on_table)
