@@ -226,6 +226,75 @@ __host__ __device__ __forceinline__ bool prune_board(u64 b, const PruneParams &p
     return thrice != 0 || sl_count >= 6 || (long long)small > p.stsl + 64 || large > p.ltc;
 }
 
+// The same predicate from per-byte tables: a board is 8 bytes of two cells
+// each, so 8 lookups give the small-tile weight (u32), and the number of copies
+// of every large value as byte-wide counters (values 0-7 in one u64, 8-15 in
+// the other; a value is counted only when it is large).  Then the large count
+// is the sum of the counters, the third-copy rule is "a chain value's counter
+// is at least 3" (0x7D added to a byte reaches 0x80 exactly at 3), and the
+// smallest_large rule is its own counter reaching 6.  About 90 operations per
+// board instead of about 220 for the per-cell loop; prune_board is the
+// definition, PruneTable the fast form (the host test checks both).
+struct PruneTable {
+    u32 small[256];
+    u64 cnt_lo[256], cnt_hi[256];
+    u64 chain_lo, chain_hi;  // 0x80 in the bytes of chain values (large, not smallest_large)
+    int sl_field;            // byte index (0-15) of smallest_large's counter, -1 if none
+    long long stsl, ltc;
+};
+
+inline void build_prune_table(const PruneParams &p, PruneTable *t)
+{
+    const long long sl = p.smallest_large;
+    const u32 small_mask = sl <= 0 ? 0u : (sl >= 14 ? 0x3FFFu : (1u << sl) - 1u);
+    const u32 large_mask = 0x3FFFu & ~small_mask;
+    const u32 sl_bit = (sl >= 0 && sl < 14) ? (1u << sl) : 0u;
+    const u32 chain_mask = large_mask & ~sl_bit;
+    for (int b = 0; b < 256; b++) {
+        u32 sm = 0;
+        u64 lo = 0, hi = 0;
+        for (int h = 0; h < 2; h++) {
+            const int x = h ? (b & 15) : (b >> 4);
+            const u32 bit = 1u << x;
+            sm += bit & small_mask;
+            if (bit & large_mask) {
+                if (x < 8) lo += 1ull << (8 * x);
+                else hi += 1ull << (8 * (x - 8));
+            }
+        }
+        t->small[b] = sm;
+        t->cnt_lo[b] = lo;
+        t->cnt_hi[b] = hi;
+    }
+    t->chain_lo = t->chain_hi = 0;
+    for (int x = 0; x < 16; x++) {
+        if (!((1u << x) & chain_mask)) continue;
+        if (x < 8) t->chain_lo |= 0x80ull << (8 * x);
+        else t->chain_hi |= 0x80ull << (8 * (x - 8));
+    }
+    t->sl_field = sl_bit ? (int)sl : -1;
+    t->stsl = p.stsl;
+    t->ltc = p.ltc;
+}
+
+__host__ __device__ __forceinline__ bool prune_by_table(u64 b, const PruneTable &t)
+{
+    u32 small = 0;
+    u64 lo = 0, hi = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const u32 byte = (u32)(b >> (8 * i)) & 0xFFu;
+        small += t.small[byte];
+        lo += t.cnt_lo[byte];
+        hi += t.cnt_hi[byte];
+    }
+    const u64 ones = 0x0101010101010101ull;
+    const int large = (int)(((lo + hi) * ones) >> 56);  // counters <= 16, their sum <= 16
+    const bool thrice = (((lo + 0x7D * ones) & t.chain_lo) | ((hi + 0x7D * ones) & t.chain_hi)) != 0;
+    const int slc = t.sl_field < 0 ? 0 : (int)(((t.sl_field < 8 ? lo : hi) >> (8 * (t.sl_field & 7))) & 0xFF);
+    return thrice || slc >= 6 || (long long)small > t.stsl + 64 || large > t.ltc;
+}
+
 // contains tile x?  (src/generate.c:89-96 returns the negation)
 __host__ __device__ __forceinline__ bool has_tile(u64 b, int x)
 {

@@ -108,7 +108,8 @@ __device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned 
 // raw move stream out of the sort (measured on LL layers: 1024 consecutive
 // inputs keep 53 % of their results).
 constexpr int MOVE_SET = 8192;
-constexpr int EXP_SMEM = TABLE_BYTES + MOVE_SET * 8;
+constexpr int PRUNE_BYTES = ((int)sizeof(PruneTable) + 15) / 16 * 16;
+constexpr int EXP_SMEM = TABLE_BYTES + MOVE_SET * 8 + PRUNE_BYTES;
 
 __device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
 {
@@ -127,8 +128,8 @@ __device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
 // PLANNED, chosen once per warp so that the choice is a uniform branch) and
 // checked against the CTA's set; returns the mask of results to write
 template <bool PLANNED>
-__device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const PruneParams &pp, const CanonPlan &plan,
-                                           unsigned long long *set, u64 r[4])
+__device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const PruneParams &pp, const PruneTable &pt,
+                                           const CanonPlan &plan, unsigned long long *set, u64 r[4])
 {
     u64 v[4];
     views(b, v);
@@ -139,7 +140,7 @@ __device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const Prune
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         u64 m;
-        if (move_left(t, v[k], &m) == 2 && !(pp.enabled && popc64(empty_mask(m)) != empties && prune_board(m, pp))) {
+        if (move_left(t, v[k], &m) == 2 && !(pp.enabled && popc64(empty_mask(m)) != empties && prune_by_table(m, pt))) {
             r[k] = PLANNED ? canon_cand(m, plan.cand(k)) : canonical(m);
             if (set_insert(set, r[k])) mask |= 1u << k;
         }
@@ -150,12 +151,17 @@ __device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const Prune
 __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 *__restrict__ in, u64 n,
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
-                                                                      PruneParams pp, u32 *err, FormationFilter ff,
-                                                                      CanonPlan plan)
+                                                                      PruneParams pp, const PruneTable *g_prune,
+                                                                      u32 *err, FormationFilter ff, CanonPlan plan)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 scan_scratch[33];
     __shared__ u64 base_sh;
+    // the prune table next to the row table; both staged before the barrier in stage_table
+    PruneTable *pt = (PruneTable *)(smem + TABLE_BYTES + MOVE_SET * 8);
+    if (pp.enabled)
+        for (int i = threadIdx.x; i < PRUNE_BYTES / 16; i += EXP_THREADS)
+            ((uint4 *)pt)[i] = __ldg((const uint4 *)g_prune + i);
     stage_table(smem, g_move);
     const RowTable t{(const unsigned short *)smem};
     unsigned long long *set = (unsigned long long *)(smem + TABLE_BYTES);
@@ -172,9 +178,9 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
         if (idx < n) {
             // boards of a formation that has reached its last layer stop here
             const bool live = !ff.fid || __ldg(ff.active + __ldg(ff.fid + fixed_pattern(b)));
-            if (live && !(pp.enabled && prune_board(b, pp))) {
-                if (planned) mask = board_moves<true>(t, b, pp, plan, set, r);
-                else mask = board_moves<false>(t, b, pp, plan, set, r);
+            if (live && !(pp.enabled && prune_by_table(b, *pt))) {
+                if (planned) mask = board_moves<true>(t, b, pp, *pt, plan, set, r);
+                else mask = board_moves<false>(t, b, pp, *pt, plan, set, r);
             }
         }
         const u32 cnt = __popc(mask);
@@ -319,10 +325,23 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     }
     if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+    // the prune table of these parameters, in device memory until they change
+    static PruneTable *d_prune = nullptr;
+    static PruneParams have{-1, -1, -1, -1};
+    if (p.enabled && (!d_prune || have.stsl != p.stsl || have.ltc != p.ltc || have.smallest_large != p.smallest_large)) {
+        static PruneTable h;
+        build_prune_table(p, &h);
+        if (!d_prune && !CGB_CUDA(cudaMalloc((void **)&d_prune, PRUNE_BYTES))) return false;
+        if (!CGB_CUDA(cudaMemcpyAsync(d_prune, &h, sizeof h, cudaMemcpyHostToDevice, s)) ||
+            !CGB_CUDA(cudaStreamSynchronize(s)))
+            return false;
+        have = p;
+    }
     const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
     kclock().begin(s, &kstats().expand_ms);
-    expand_moves_kernel<<<grid, EXP_THREADS, EXP_SMEM, s>>>(in, n, out, cap, c.d, t.move, p, c.err, ff, plan);
+    expand_moves_kernel<<<grid, EXP_THREADS, EXP_SMEM, s>>>(in, n, out, cap, c.d, t.move, p, d_prune, c.err, ff,
+                                                            plan);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;

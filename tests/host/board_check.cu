@@ -1,7 +1,7 @@
 // Host-side check of the board algebra in cablegen_b200/csrc/board.cuh: reads
 // boards (u64, raw) from argv[1] and prune parameter sets "stsl,ltc,sl" from
-// argv[2..], writes one byte per (parameter set, board) with prune_board's
-// verdict to stdout.
+// argv[2..], writes one byte per (parameter set, board) to stdout: bit 0 the
+// verdict of prune_board, bit 1 that of prune_by_table (the table-driven form).
 #include "../../cablegen_b200/csrc/board.cuh"
 #include <cstdio>
 #include <cstdlib>
@@ -20,8 +20,11 @@ int main(int argc, char **argv)
         long long stsl, ltc, sl;
         if (std::sscanf(argv[a], "%lld,%lld,%lld", &stsl, &ltc, &sl) != 3) return 2;
         cgb::PruneParams p{stsl, ltc, sl, 1};
+        static cgb::PruneTable t;
+        cgb::build_prune_table(p, &t);
         std::vector<unsigned char> out(b.size());
-        for (size_t i = 0; i < b.size(); i++) out[i] = cgb::prune_board(b[i], p) ? 1 : 0;
+        for (size_t i = 0; i < b.size(); i++)
+            out[i] = (cgb::prune_board(b[i], p) ? 1 : 0) | (cgb::prune_by_table(b[i], t) ? 2 : 0);
         std::fwrite(out.data(), 1, out.size(), stdout);
     }
     return 0;
