@@ -205,70 +205,45 @@ struct SpawnSums {
 // so a thread keeps up to eight independent loads in flight.
 constexpr int DIRECT_THREADS = 1024;
 
-// A probe in two halves, so that the loads of several probes (of both tables)
-// are in flight before any is resolved: probe_issue computes the home slots
-// and loads them (nothing for an illegal move or, for 8-byte slots, a key
-// whose constant bytes differ); probe_finish reads the value or 0, and walks
-// on in the rare case that the home slot holds another key.
-template <typename V, int N>
-__device__ __forceinline__ void probe_issue(const DevTable<V> &t, const u64 *key, u32 legal, u64 *w0, u64 *w1,
-                                            u64 *slot, u32 *tag)
+template <typename V>
+__device__ __forceinline__ void probe4(const DevTable<V> &t, const u64 *key, u32 legal, V *out)
 {
     if (t.kind == INDEX_HASH && t.ch.on) {
+        u64 h[4], e[4];
+        u32 tag[4];
 #pragma unroll
-        for (int j = 0; j < N; j++) {
-            const bool on = ((legal >> j) & 1u) && (key[j] & t.ch.cmask) == t.ch.cval;
-            slot[j] = compact_home(t.ch, key[j], &tag[j]);
-            w0[j] = on ? __ldg((const u64 *)t.slots + slot[j]) : 0ull;
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && (key[j] & t.ch.cmask) == t.ch.cval;
+            h[j] = compact_home(t.ch, key[j], &tag[j]);
+            e[j] = on ? __ldg((const u64 *)t.slots + h[j]) : 0ull;
         }
-    } else if (t.kind == INDEX_HASH) {
 #pragma unroll
-        for (int j = 0; j < N; j++) {
-            const bool on = ((legal >> j) & 1u) && t.cap;
-            slot[j] = on ? home_slot(key[j], t.cap) : 0;
-            const ulonglong2 e = on ? __ldg(t.slots + slot[j]) : make_ulonglong2(0, 0);
-            w0[j] = e.x;
-            w1[j] = e.y;
+        for (int j = 0; j < 4; j++) {
+            if ((u32)e[j] == tag[j]) out[j] = from_bits<V>(e[j] >> 32);
+            else if ((u32)e[j] == 0u) out[j] = V(0);
+            else out[j] = compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, h[j], tag[j]);
         }
+        return;
     }
-}
-
-template <typename V, int N>
-__device__ __forceinline__ void probe_finish(const DevTable<V> &t, const u64 *key, u32 legal, const u64 *w0,
-                                             const u64 *w1, const u64 *slot, const u32 *tag, V *out)
-{
-    if (t.kind == INDEX_HASH && t.ch.on) {
+    if (t.kind == INDEX_HASH) {
+        u64 s[4];
+        ulonglong2 e[4];
 #pragma unroll
-        for (int j = 0; j < N; j++) {
-            if ((u32)w0[j] == tag[j]) out[j] = from_bits<V>(w0[j] >> 32);
-            else if ((u32)w0[j] == 0u) out[j] = V(0);
-            else out[j] = compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, slot[j], tag[j]);
+        for (int j = 0; j < 4; j++) {
+            const bool on = (legal >> j) & 1 && t.cap;
+            s[j] = on ? home_slot(key[j], t.cap) : 0;
+            e[j] = on ? __ldg(t.slots + s[j]) : make_ulonglong2(0, 0);
         }
-    } else if (t.kind == INDEX_HASH) {
 #pragma unroll
-        for (int j = 0; j < N; j++) {
-            if (!((legal >> j) & 1u) || w0[j] == 0) out[j] = V(0);
-            else if (w0[j] == key[j]) out[j] = from_bits<V>(w1[j]);
-            else out[j] = hash_probe_rest<V>(t.slots, t.cap, key[j], slot[j]);
+        for (int j = 0; j < 4; j++) {
+            if (!((legal >> j) & 1) || e[j].x == 0) out[j] = V(0);
+            else if (e[j].x == key[j]) out[j] = from_bits<V>(e[j].y);
+            else out[j] = hash_probe_rest<V>(t.slots, t.cap, key[j], s[j]);
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < N; j++) out[j] = ((legal >> j) & 1u) ? sorted_lookup(t, key[j]) : V(0);
+        for (int j = 0; j < 4; j++) out[j] = ((legal >> j) & 1) ? sorted_lookup(t, key[j]) : V(0);
     }
-}
-
-// N successors looked up in the s+2 table and N in the s+4 table, all loads
-// issued before any is resolved
-template <typename V, int N>
-__device__ __forceinline__ void probe_both(const DevTable<V> &t2, const u64 *k2, u32 l2, V *p2,
-                                           const DevTable<V> &t4, const u64 *k4, u32 l4, V *p4)
-{
-    u64 a0[N], a1[N], as[N], b0[N], b1[N], bs[N];
-    u32 at[N], bt[N];
-    probe_issue<V, N>(t2, k2, l2, a0, a1, as, at);
-    probe_issue<V, N>(t4, k4, l4, b0, b1, bs, bt);
-    probe_finish<V, N>(t2, k2, l2, a0, a1, as, at, p2);
-    probe_finish<V, N>(t4, k4, l4, b0, b1, bs, bt, p4);
 }
 
 // The best values of one empty cell: its eight successors (2 and 4 spawned
@@ -294,23 +269,42 @@ __device__ __forceinline__ void cell_bests(const RowTable &rt, const u64 v[4], i
     }
     probes += __popc(l2) + __popc(l4);
     V p2[4], p4[4];
-    {  // one table at a time: all of a table's loads in flight, fewer live registers
-        u64 w0[4], w1[4], sl[4];
-        u32 tg[4];
-        probe_issue<V, 4>(t2, k2, l2, w0, w1, sl, tg);
-        probe_finish<V, 4>(t2, k2, l2, w0, w1, sl, tg, p2);
-        probe_issue<V, 4>(t4, k4, l4, w0, w1, sl, tg);
-        probe_finish<V, 4>(t4, k4, l4, w0, w1, sl, tg, p4);
-    }
+    probe4(t2, k2, l2, p2);
+    probe4(t4, k4, l4, p4);
     best2 = vmax(vmax(p2[0], p2[1]), vmax(p2[2], p2[3]));
     best4 = vmax(vmax(p4[0], p4[1]), vmax(p4[2], p4[3]));
 }
 
-// cell_bests with the four views in a loop that is not unrolled: STEP views'
-// successors per iteration (2 x STEP loads in flight per lane, hidden by the
-// other warps), a fraction of the code.  The unrolled body of all eight
+// One probe of a table (the successor is looked up only when its move was legal).
+template <typename V>
+__device__ __forceinline__ V probe1(const DevTable<V> &t, u64 key, bool legal)
+{
+    if (!legal) return V(0);
+    if (t.kind == INDEX_HASH && t.ch.on) {
+        if ((key & t.ch.cmask) != t.ch.cval) return V(0);
+        u32 tag0;
+        const u64 h = compact_home(t.ch, key, &tag0);
+        const u64 e = __ldg((const u64 *)t.slots + h);
+        if ((u32)e == tag0) return from_bits<V>(e >> 32);
+        if ((u32)e == 0u) return V(0);
+        return compact_probe_rest<V>((const u64 *)t.slots, t.cap, t.ch.dbits, h, tag0);
+    }
+    if (t.kind == INDEX_HASH) {
+        if (t.cap == 0) return V(0);
+        const u64 s = home_slot(key, t.cap);
+        const ulonglong2 e = __ldg(t.slots + s);
+        if (e.x == key) return from_bits<V>(e.y);
+        if (e.x == 0) return V(0);
+        return hash_probe_rest<V>(t.slots, t.cap, key, s);
+    }
+    return sorted_lookup(t, key);
+}
+
+// cell_bests with the four views in a loop that is not unrolled: one view's
+// two successors per iteration (two loads in flight per lane, hidden by the
+// other warps), a quarter of the code.  The unrolled body of all eight
 // successors is large enough that warps wait on instruction fetch.
-template <bool PLANNED, int STEP, typename V>
+template <bool PLANNED, typename V>
 __device__ __forceinline__ void cell_bests_rolled(const RowTable &rt, u64 b, int cell, const CanonPlan &plan,
                                                   const DevTable<V> &t2, const DevTable<V> &t4, V &best2, V &best4,
                                                   u32 &probes)
@@ -320,32 +314,21 @@ __device__ __forceinline__ void cell_bests_rolled(const RowTable &rt, u64 b, int
     best2 = V(0);
     best4 = V(0);
 #pragma unroll 1
-    for (int k0 = 0; k0 < 4; k0 += STEP) {
-        u64 c2[STEP], c4[STEP];
-        u32 l2 = 0, l4 = 0;
-#pragma unroll
-        for (int j = 0; j < STEP; j++) {
-            // view k: id, H, T, H.T; the cell of the spawn in it
-            const int k = k0 + j;
-            const Half x = (k & 2) ? t : h;
-            const u64 y = (k & 1) ? whole(flip_h(x)) : whole(x);
-            const int row = (k & 2) ? q0 : r0;
-            const int col = ((k & 2) ? r0 : q0) ^ ((k & 1) ? 3 : 0);
-            const int sh = 60 - 4 * (4 * row + col);
-            u64 m2, m4;
-            if (move_left(rt, y | (1ull << sh), &m2) == 2) l2 |= 1u << j;
-            if (move_left(rt, y | (2ull << sh), &m4) == 2) l4 |= 1u << j;
-            c2[j] = PLANNED ? canon_cand(m2, plan.cand(k)) : canonical(m2);
-            c4[j] = PLANNED ? canon_cand(m4, plan.cand(k)) : canonical(m4);
-        }
-        probes += __popc(l2) + __popc(l4);
-        V p2[STEP], p4[STEP];
-        probe_both<V, STEP>(t2, c2, l2, p2, t4, c4, l4, p4);
-#pragma unroll
-        for (int j = 0; j < STEP; j++) {
-            best2 = vmax(best2, p2[j]);
-            best4 = vmax(best4, p4[j]);
-        }
+    for (int k = 0; k < 4; k++) {
+        // view k: id, H, T, H.T; the cell of the spawn in it
+        const Half x = (k & 2) ? t : h;
+        const u64 y = (k & 1) ? whole(flip_h(x)) : whole(x);
+        const int row = (k & 2) ? q0 : r0;
+        const int col = ((k & 2) ? r0 : q0) ^ ((k & 1) ? 3 : 0);
+        const int sh = 60 - 4 * (4 * row + col);
+        u64 m2, m4;
+        const bool ok2 = move_left(rt, y | (1ull << sh), &m2) == 2;
+        const bool ok4 = move_left(rt, y | (2ull << sh), &m4) == 2;
+        const u64 c2 = PLANNED ? canon_cand(m2, plan.cand(k)) : canonical(m2);
+        const u64 c4 = PLANNED ? canon_cand(m4, plan.cand(k)) : canonical(m4);
+        probes += (u32)ok2 + (u32)ok4;
+        best2 = vmax(best2, probe1(t2, c2, ok2));
+        best4 = vmax(best4, probe1(t4, c4, ok4));
     }
 }
 
@@ -397,11 +380,13 @@ __global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u
 // views), canonicalises them over the images its CanonPlan allows, probes the
 // s+2 and s+4 tables, and leaves the two best values in shared memory; the
 // owning lane then adds its pairs' values in cell order.
+constexpr int ITEM_THREADS = 1024;
+constexpr int ITEM_WARPS = ITEM_THREADS / 32;
 constexpr int ITEM_MAX = 32 * 16;  // pairs of 32 boards at most
-template <typename V, int THREADS>
-constexpr int item_smem() { return TABLE_BYTES_S + (THREADS / 32) * (ITEM_MAX * 2 + 2 * 32 * (int)sizeof(V)); }
+template <typename V>
+constexpr int item_smem() { return TABLE_BYTES_S + ITEM_WARPS * (ITEM_MAX * 2 + 2 * 32 * (int)sizeof(V)); }
 
-template <typename V, int STEP, int ITEM_THREADS>
+template <typename V>
 __global__ void __launch_bounds__(ITEM_THREADS, 1)
     solve_items_kernel(const u64 *__restrict__ keys, u64 n, V *__restrict__ out, DevTable<V> t2, DevTable<V> t4,
                        SolveRules r, const unsigned short *g_move, u64 *probes_out, CanonPlan plan)
@@ -411,7 +396,7 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
     const RowTable rt{(const unsigned short *)smem};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned short *items = (unsigned short *)(smem + TABLE_BYTES_S) + warp * ITEM_MAX;  // (lane << 4) | cell
-    V *best_sh = (V *)(smem + TABLE_BYTES_S + (ITEM_THREADS / 32) * ITEM_MAX * 2) + warp * 64;   // [2][32]
+    V *best_sh = (V *)(smem + TABLE_BYTES_S + ITEM_WARPS * ITEM_MAX * 2) + warp * 64;   // [2][32]
     u32 probes = 0;
     const u64 stride = (u64)gridDim.x * ITEM_THREADS;
     for (u64 base = (u64)blockIdx.x * ITEM_THREADS + warp * 32; base < n; base += stride) {
@@ -442,8 +427,8 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
             const u64 ob = __shfl_sync(0xffffffffu, b, owner);
             V best2 = 0, best4 = 0;
             if (has) {
-                if (planned) cell_bests_rolled<true, STEP>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
-                else cell_bests_rolled<false, STEP>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
+                if (planned) cell_bests_rolled<true>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
+                else cell_bests_rolled<false>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
             }
             best_sh[lane] = best2;
             best_sh[32 + lane] = best4;
@@ -681,24 +666,16 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     return t;
 }
 
-// 0: direct (one thread per board), 1: (board, cell) pairs per warp, one view's
-// successors per step, 2: the same, two views' successors per step, 3: as 2
-// with 768-thread CTAs (more registers per thread)
-int g_solve_variant = 1;
-
-template <typename V, int STEP, int THREADS>
-static bool item_attr()
-{
-    return CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<V, STEP, THREADS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, item_smem<V, THREADS>()));
-}
+int g_solve_variant = 1;  // 0: direct (one thread per board), 1: (board, cell) pairs per warp
 
 static bool solve_attrs()
 {
     static bool attr = false;
     if (!attr) {
-        if (!item_attr<double, 1, 1024>() || !item_attr<float, 1, 1024>() || !item_attr<double, 2, 1024>() ||
-            !item_attr<float, 2, 1024>() || !item_attr<double, 2, 768>() || !item_attr<float, 2, 768>() ||
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           item_smem<double>())) ||
+            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           item_smem<float>())) ||
             !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<double>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_BYTES_S)) ||
             !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<float>,
@@ -716,13 +693,7 @@ static void enqueue_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, 
                           const CanonPlan &plan)
 {
     if (g_solve_variant == 1)
-        solve_items_kernel<V, 1, 1024><<<grid_for(n, 1024, 1), 1024, item_smem<V, 1024>(), s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
-    else if (g_solve_variant == 2)
-        solve_items_kernel<V, 2, 1024><<<grid_for(n, 1024, 1), 1024, item_smem<V, 1024>(), s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
-    else if (g_solve_variant == 3)
-        solve_items_kernel<V, 2, 768><<<grid_for(n, 768, 1), 768, item_smem<V, 768>(), s>>>(
+        solve_items_kernel<V><<<grid_for(n, ITEM_THREADS, 1), ITEM_THREADS, item_smem<V>(), s>>>(
             keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
     else
         solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(

@@ -116,7 +116,7 @@ def test_batch_knobs_do_not_change_results(cuda, batch_case):
     names = ("sort_variant", "solve_variant", "hash_load_pct")
     old = {k: cuda.get_option(k) for k in names}
     try:
-        for sv, so, hl in ((2, 1, 60), (0, 0, 25), (3, 2, 45), (4, 3, 0)):
+        for sv, so, hl in ((2, 1, 60), (0, 0, 25), (3, 1, 45), (4, 0, 0)):
             cuda.set_option("sort_variant", sv)
             cuda.set_option("solve_variant", so)
             cuda.set_option("hash_load_pct", hl)
