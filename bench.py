@@ -570,6 +570,9 @@ def run_ours(args):
                                 "share": round(kst[f"{k}_ms"] / max(dev_ms, 1e-9), 4)}
                             for k in fams}}
     roofline["kernels"]["solve"]["lookups"] = kst["lookups"]
+    # the move results the expansion found and the ones left after its per-block set
+    roofline["kernels"]["expand"]["moves_raw"] = kst["moves_raw"]
+    roofline["kernels"]["expand"]["moves_kept"] = kst["moves_kept"]
     roofline["kernels"]["index"] = {"ms": round(kst["index_ms"], 3), "GB/s": None,
                                     "share": round(kst["index_ms"] / max(dev_ms, 1e-9), 4),
                                     "builds": kst["index_builds"]}

@@ -46,6 +46,7 @@ struct KernelStats {
         spawn_bytes = 0, solve_bytes = 0;
     u64 onesweep_launches = 0, solve_launches = 0, solve_boards = 0, lookups = 0;
     u64 index_builds = 0, compact_index_builds = 0;
+    u64 moves_raw = 0, moves_kept = 0;  // move results before / after the per-block set
 };
 KernelStats &kstats();
 

@@ -129,7 +129,7 @@ __device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
 // checked against the CTA's set; returns the mask of results to write
 template <bool PLANNED>
 __device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const PruneParams &pp, const PruneTable &pt,
-                                           const CanonPlan &plan, unsigned long long *set, u64 r[4])
+                                           const CanonPlan &plan, unsigned long long *set, u64 r[4], u32 *raw)
 {
     u64 v[4];
     views(b, v);
@@ -142,6 +142,7 @@ __device__ __forceinline__ u32 board_moves(const RowTable &t, u64 b, const Prune
         u64 m;
         if (move_left(t, v[k], &m) == 2 && !(pp.enabled && popc64(empty_mask(m)) != empties && prune_by_table(m, pt))) {
             r[k] = PLANNED ? canon_cand(m, plan.cand(k)) : canonical(m);
+            (*raw)++;
             if (set_insert(set, r[k])) mask |= 1u << k;
         }
     }
@@ -152,7 +153,8 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
                                                                       u64 *__restrict__ out, u64 cap,
                                                                       u64 *out_count, const unsigned short *g_move,
                                                                       PruneParams pp, const PruneTable *g_prune,
-                                                                      u32 *err, FormationFilter ff, CanonPlan plan)
+                                                                      u32 *err, FormationFilter ff, CanonPlan plan,
+                                                                      u64 *raw_count)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 scan_scratch[33];
@@ -166,6 +168,7 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
     const RowTable t{(const unsigned short *)smem};
     unsigned long long *set = (unsigned long long *)(smem + TABLE_BYTES);
     const u64 stride = (u64)gridDim.x * EXP_THREADS;
+    u32 raw = 0;  // legal, unpruned moves before the set drops repeats
     for (u64 first = (u64)blockIdx.x * EXP_THREADS; first < n; first += stride) {
         for (int i = threadIdx.x; i < MOVE_SET; i += EXP_THREADS) set[i] = 0ull;
         __syncthreads();
@@ -179,8 +182,8 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
             // boards of a formation that has reached its last layer stop here
             const bool live = !ff.fid || __ldg(ff.active + __ldg(ff.fid + fixed_pattern(b)));
             if (live && !(pp.enabled && prune_by_table(b, *pt))) {
-                if (planned) mask = board_moves<true>(t, b, pp, *pt, plan, set, r);
-                else mask = board_moves<false>(t, b, pp, *pt, plan, set, r);
+                if (planned) mask = board_moves<true>(t, b, pp, *pt, plan, set, r, &raw);
+                else mask = board_moves<false>(t, b, pp, *pt, plan, set, r, &raw);
             }
         }
         const u32 cnt = __popc(mask);
@@ -197,6 +200,8 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
                 if (mask & (1u << k)) out[pos++] = r[k];
         }
     }
+    const u32 w = __reduce_add_sync(0xffffffffu, raw);
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd((unsigned long long *)raw_count, (unsigned long long)w);
 }
 
 __global__ void __launch_bounds__(256) count_spawns_kernel(const u64 *__restrict__ in, u64 n, u64 *total)
@@ -285,7 +290,8 @@ static bool read_word(u64 *dst, const u64 *src, cudaStream_t s)
 
 // one copy for a count word and the error word (Counters keeps the error word
 // 32 words after the counts)
-static bool read_count_checked(u64 *dst, Counters &c, int idx, cudaStream_t s, const char *what)
+static bool read_count_checked(u64 *dst, Counters &c, int idx, cudaStream_t s, const char *what,
+                               u64 *raw = nullptr)
 {
     u64 words[33];
     if (!CGB_CUDA(cudaMemcpyAsync(words, c.d, sizeof words, cudaMemcpyDeviceToHost, s))) return false;
@@ -296,6 +302,7 @@ static bool read_count_checked(u64 *dst, Counters &c, int idx, cudaStream_t s, c
         return false;
     }
     *dst = words[idx];
+    if (raw) *raw = words[5];
     return true;
 }
 
@@ -324,6 +331,7 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
         attr = true;
     }
     if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(c.d + 5, 0, sizeof(u64), s))) return false;
     if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
     // the prune table of these parameters, in device memory until they change
     static PruneTable *d_prune = nullptr;
@@ -341,12 +349,15 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
     const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
     kclock().begin(s, &kstats().expand_ms);
     expand_moves_kernel<<<grid, EXP_THREADS, EXP_SMEM, s>>>(in, n, out, cap, c.d, t.move, p, d_prune, c.err, ff,
-                                                            plan);
+                                                            plan, c.d + 5);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    if (!read_count_checked(n_out, c, 0, s, "expand_moves")) return false;
+    u64 raw = 0;
+    if (!read_count_checked(n_out, c, 0, s, "expand_moves", &raw)) return false;
     kclock().flush();
     kstats().expand_bytes += 8 * (n + *n_out);
+    kstats().moves_raw += raw;
+    kstats().moves_kept += *n_out;
     return true;
 }
 

@@ -80,6 +80,8 @@ int cgb_get_kernel_stats(cgb_kernel_stats *o)
     o->lookups = k.lookups;
     o->index_builds = k.index_builds;
     o->compact_index_builds = k.compact_index_builds;
+    o->moves_raw = k.moves_raw;
+    o->moves_kept = k.moves_kept;
     return 0;
 }
 
