@@ -9,7 +9,7 @@ The knobs (cgb_set_option):
   from the one 32-bit word that holds them), 4 the same with 8192-key tiles of 512 threads (the
   tile-size knob);
 * ``solve_variant`` -- 0 one thread per board, 1 the (board, empty cell) pairs of 32 boards
-  spread over a warp, 2 the same with each view's probes prefetched into L2 one view ahead;
+  spread over a warp;
 * ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
   table size; a higher load means more probes, a lower one more memory and a lower L2 hit
   rate).
@@ -32,7 +32,7 @@ from . import configs, device
 
 KNOBS = {
     "sort_variant": [4, 3, 1, 0, 2],
-    "solve_variant": [1, 2, 0],
+    "solve_variant": [1, 0],
     "hash_load_pct": [0, 25, 45],
 }
 

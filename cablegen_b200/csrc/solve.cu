@@ -332,71 +332,6 @@ __device__ __forceinline__ void cell_bests_rolled(const RowTable &rt, u64 b, int
     }
 }
 
-// address of the slot a probe reads first (nullptr: no load needed)
-template <typename V>
-__device__ __forceinline__ const void *probe_address(const DevTable<V> &t, u64 key, bool legal)
-{
-    if (!legal) return nullptr;
-    if (t.kind == INDEX_HASH && t.ch.on) {
-        if ((key & t.ch.cmask) != t.ch.cval) return nullptr;
-        u32 tag0;
-        return (const u64 *)t.slots + compact_home(t.ch, key, &tag0);
-    }
-    if (t.kind == INDEX_HASH) return t.cap ? (const void *)(t.slots + home_slot(key, t.cap)) : nullptr;
-    return nullptr;  // sorted layers: a bisection, nothing to fetch ahead
-}
-
-__device__ __forceinline__ void prefetch_l2(const void *p)
-{
-    if (p) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
-// cell_bests_rolled, software-pipelined by one view: each step forms view k's
-// two successors and prefetches their slots into L2 (no register holds a
-// prefetch in flight), then probes view k-1's successors, whose slots were
-// prefetched one step -- two moves and two canonical forms -- earlier.
-template <bool PLANNED, typename V>
-__device__ __forceinline__ void cell_bests_piped(const RowTable &rt, u64 b, int cell, const CanonPlan &plan,
-                                                 const DevTable<V> &t2, const DevTable<V> &t4, V &best2, V &best4,
-                                                 u32 &probes)
-{
-    const Half h = halves(b), t = transpose(h);
-    const int r0 = cell >> 2, q0 = cell & 3;
-    best2 = V(0);
-    best4 = V(0);
-    u64 c2 = 0, c4 = 0;
-    bool ok2 = false, ok4 = false;
-#pragma unroll 1
-    for (int k = 0; k <= 4; k++) {
-        u64 n2 = 0, n4 = 0;
-        bool nok2 = false, nok4 = false;
-        if (k < 4) {
-            // view k: id, H, T, H.T; the cell of the spawn in it
-            const Half x = (k & 2) ? t : h;
-            const u64 y = (k & 1) ? whole(flip_h(x)) : whole(x);
-            const int row = (k & 2) ? q0 : r0;
-            const int col = ((k & 2) ? r0 : q0) ^ ((k & 1) ? 3 : 0);
-            const int sh = 60 - 4 * (4 * row + col);
-            u64 m2, m4;
-            nok2 = move_left(rt, y | (1ull << sh), &m2) == 2;
-            nok4 = move_left(rt, y | (2ull << sh), &m4) == 2;
-            n2 = PLANNED ? canon_cand(m2, plan.cand(k)) : canonical(m2);
-            n4 = PLANNED ? canon_cand(m4, plan.cand(k)) : canonical(m4);
-            prefetch_l2(probe_address(t2, n2, nok2));
-            prefetch_l2(probe_address(t4, n4, nok4));
-        }
-        if (k > 0) {
-            probes += (u32)ok2 + (u32)ok4;
-            best2 = vmax(best2, probe1(t2, c2, ok2));
-            best4 = vmax(best4, probe1(t4, c4, ok4));
-        }
-        c2 = n2;
-        c4 = n4;
-        ok2 = nok2;
-        ok4 = nok4;
-    }
-}
-
 template <typename V>
 __global__ void __launch_bounds__(DIRECT_THREADS, 1) solve_direct_kernel(const u64 *__restrict__ keys, u64 n,
                                                                          V *__restrict__ out, DevTable<V> t2,
@@ -451,7 +386,7 @@ constexpr int ITEM_MAX = 32 * 16;  // pairs of 32 boards at most
 template <typename V>
 constexpr int item_smem() { return TABLE_BYTES_S + ITEM_WARPS * (ITEM_MAX * 2 + 2 * 32 * (int)sizeof(V)); }
 
-template <typename V, bool PIPED>
+template <typename V>
 __global__ void __launch_bounds__(ITEM_THREADS, 1)
     solve_items_kernel(const u64 *__restrict__ keys, u64 n, V *__restrict__ out, DevTable<V> t2, DevTable<V> t4,
                        SolveRules r, const unsigned short *g_move, u64 *probes_out, CanonPlan plan)
@@ -492,13 +427,8 @@ __global__ void __launch_bounds__(ITEM_THREADS, 1)
             const u64 ob = __shfl_sync(0xffffffffu, b, owner);
             V best2 = 0, best4 = 0;
             if (has) {
-                if (PIPED) {
-                    if (planned) cell_bests_piped<true>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
-                    else cell_bests_piped<false>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
-                } else {
-                    if (planned) cell_bests_rolled<true>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
-                    else cell_bests_rolled<false>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
-                }
+                if (planned) cell_bests_rolled<true>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
+                else cell_bests_rolled<false>(rt, ob, cell, plan, t2, t4, best2, best4, probes);
             }
             best_sh[lane] = best2;
             best_sh[32 + lane] = best4;
@@ -736,21 +666,15 @@ static DevTable<V> dev_table(const LayerIndex &ix)
     return t;
 }
 
-// 0: direct (one thread per board), 1: (board, cell) pairs per warp, 2: as 1
-// with the probes of each view prefetched into L2 one view ahead
-int g_solve_variant = 1;
+int g_solve_variant = 1;  // 0: direct (one thread per board), 1: (board, cell) pairs per warp
 
 static bool solve_attrs()
 {
     static bool attr = false;
     if (!attr) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<double, false>,
+        if (!CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<double>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, item_smem<double>())) ||
-            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<float, false>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, item_smem<float>())) ||
-            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<double, true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, item_smem<double>())) ||
-            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<float, true>,
+            !CGB_CUDA(cudaFuncSetAttribute(solve_items_kernel<float>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, item_smem<float>())) ||
             !CGB_CUDA(cudaFuncSetAttribute(solve_direct_kernel<double>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, TABLE_BYTES_S)) ||
@@ -769,10 +693,7 @@ static void enqueue_solve(const u64 *keys, u64 n, V *out, const LayerIndex &t2, 
                           const CanonPlan &plan)
 {
     if (g_solve_variant == 1)
-        solve_items_kernel<V, false><<<grid_for(n, ITEM_THREADS, 1), ITEM_THREADS, item_smem<V>(), s>>>(
-            keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
-    else if (g_solve_variant == 2)
-        solve_items_kernel<V, true><<<grid_for(n, ITEM_THREADS, 1), ITEM_THREADS, item_smem<V>(), s>>>(
+        solve_items_kernel<V><<<grid_for(n, ITEM_THREADS, 1), ITEM_THREADS, item_smem<V>(), s>>>(
             keys, n, out, dev_table<V>(t2), dev_table<V>(t4), r, rt.move, probes, plan);
     else
         solve_direct_kernel<V><<<grid_for(n, DIRECT_THREADS, 1), DIRECT_THREADS, TABLE_BYTES_S, s>>>(

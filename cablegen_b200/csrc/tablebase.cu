@@ -101,9 +101,8 @@ int cgb_set_option(const char *name, long long value)
         }
         E().index_kind = (int)value;
     } else if (k == "solve_variant") {
-        if (value < 0 || value > 2) {
-            set_error("cgb_set_option: solve_variant must be 0 (one thread per board), 1 (board-cell pairs) or 2 "
-                      "(board-cell pairs, probes prefetched one view ahead)");
+        if (value < 0 || value > 1) {
+            set_error("cgb_set_option: solve_variant must be 0 (one thread per board) or 1 (board-cell pairs)");
             return -1;
         }
         g_solve_variant = (int)value;

@@ -107,13 +107,13 @@ def test_solve_variants_agree(cuda, precision, name, end):
     old = cuda.get_option("solve_variant")
     got = {}
     try:
-        for v in (0, 1, 2):
+        for v in (0, 1):
             cuda.set_option("solve_variant", v)
             _, got[v], _ = cuda.tablebase(f.initial, f.start, f.end_gen, 0, f.winstates, precision=precision,
                                           keep_tables=True)
     finally:
         cuda.set_option("solve_variant", old)
-    for v in (0, 2):
+    for v in (0,):
         for s in got[1]:
             assert np.array_equal(got[v][s][1], got[1][s][1]), (v, s)
     if precision == 64 and end is None:
