@@ -518,6 +518,104 @@ __global__ void compact_build_kernel(const u64 *__restrict__ keys, const float *
     }
 }
 
+// ---- region-partitioned build of the 16-byte-slot index ----------------------
+// The atomic build inserts every key with a compare-and-swap on a random slot of
+// a table that was zeroed first: a random read-modify-write per key.  This form
+// partitions the keys by region of their home slot (2048 slots = 32 KiB), builds
+// each region in shared memory and writes it out whole: the table is written
+// once, sequentially, and never zeroed.  A key whose linear probe runs past its
+// region's end goes to an overflow list, inserted afterwards into the finished
+// table with the atomic probe; slots from its home to the region's end are all
+// taken, so the probe order of linear probing is kept.
+constexpr u32 BUILD_REGION = 2048;
+
+__global__ void region_count_kernel(const u64 *__restrict__ keys, u64 n, u64 cap, u32 *counts)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+        atomicAdd(counts + home_slot(keys[i], cap) / BUILD_REGION, 1u);
+}
+
+// exclusive scan of `counts` into `offsets` (nreg + 1 entries), one CTA of 1024 threads
+__global__ void __launch_bounds__(1024) region_scan_kernel(const u32 *counts, u32 nreg, u32 *offsets)
+{
+    __shared__ u32 scratch[33];
+    u32 carry = 0;
+    for (u32 base = 0; base < nreg; base += 1024) {
+        const u32 i = base + threadIdx.x;
+        const u32 v = i < nreg ? counts[i] : 0u;
+        u32 total;
+        const u32 ex = block_exclusive_scan<u32>(v, scratch, &total);
+        if (i < nreg) offsets[i] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) offsets[nreg] = carry;
+}
+
+template <typename V>
+__global__ void region_scatter_kernel(const u64 *__restrict__ keys, const V *__restrict__ vals, u64 n, u64 cap,
+                                      const u32 *__restrict__ offsets, u32 *cursor, ulonglong2 *tmp)
+{
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
+        const u64 key = keys[i];
+        const u32 r = (u32)(home_slot(key, cap) / BUILD_REGION);
+        const u32 p = offsets[r] + atomicAdd(cursor + r, 1u);
+        tmp[p] = make_ulonglong2(key, to_bits<V>(vals[i]));
+    }
+}
+
+__global__ void __launch_bounds__(512) region_build_kernel(const ulonglong2 *__restrict__ tmp,
+                                                           const u32 *__restrict__ offsets, u32 nreg, u64 cap,
+                                                           ulonglong2 *slots, ulonglong2 *overflow, u32 max_over,
+                                                           u32 *n_over, u32 *err)
+{
+    __shared__ ulonglong2 tab[BUILD_REGION];
+    for (u32 r = blockIdx.x; r < nreg; r += gridDim.x) {
+        for (u32 j = threadIdx.x; j < BUILD_REGION; j += blockDim.x) tab[j] = make_ulonglong2(0, 0);
+        __syncthreads();
+        const u64 base = (u64)r * BUILD_REGION;
+        const u32 len = (u32)min((u64)BUILD_REGION, cap - base);
+        for (u32 j = offsets[r] + threadIdx.x; j < offsets[r + 1]; j += blockDim.x) {
+            const ulonglong2 e = tmp[j];
+            bool placed = false;
+            for (u32 sl = (u32)(home_slot(e.x, cap) - base); sl < len; sl++) {
+                if (atomicCAS((unsigned long long *)&tab[sl].x, 0ull, (unsigned long long)e.x) == 0ull) {
+                    tab[sl].y = e.y;
+                    placed = true;
+                    break;
+                }
+            }
+            if (!placed) {
+                const u32 k = atomicAdd(n_over, 1u);
+                if (k < max_over) overflow[k] = e;
+                else atomicOr(err, ERR_CAPACITY);
+            }
+        }
+        __syncthreads();
+        for (u32 j = threadIdx.x; j < len; j += blockDim.x) slots[base + j] = tab[j];
+        __syncthreads();
+    }
+}
+
+// the overflow keys, inserted into the finished table by the atomic linear probe
+__global__ void overflow_insert_kernel(const ulonglong2 *__restrict__ over, u32 n, ulonglong2 *slots, u64 cap,
+                                       u32 *err)
+{
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const ulonglong2 e = over[i];
+        u64 s = home_slot(e.x, cap);
+        bool placed = false;
+        for (u64 p = 0; p < cap; p++) {
+            if (atomicCAS((unsigned long long *)&slots[s].x, 0ull, (unsigned long long)e.x) == 0ull) {
+                slots[s].y = e.y;
+                placed = true;
+                break;
+            }
+            s = (s + 1 == cap) ? 0 : s + 1;
+        }
+        if (!placed) atomicOr(err, ERR_CAPACITY);
+    }
+}
+
 static int grid_for(u64 n, int threads, int per_sm)
 {
     int dev = 0, sms = 0;
@@ -581,6 +679,68 @@ static bool build_compact(LayerIndex &ix, IndexStorage &st, Counters &c, cudaStr
     return true;
 }
 
+int g_region_build = 1;  // 16-byte-slot indexes of 2^16..2^28 keys built region by region
+
+// the region-partitioned build (above); leaves ix.kind == INDEX_BISECT when the
+// overflow list ran out (the caller then builds with the atomic form)
+static bool build_regions(LayerIndex &ix, int vbytes, IndexStorage &st, Counters &c, cudaStream_t s)
+{
+    const u64 n = ix.n;
+    const u64 cap = hash_capacity(n);
+    const u32 nreg = (u32)((cap + BUILD_REGION - 1) / BUILD_REGION);
+    const u32 max_over = (u32)(n / 32 + 4096);
+    if (!ensure_storage(st, cap * 16, s)) return false;
+    // scratch: counts, cursors, offsets (u32), the scattered pairs, the overflow list
+    const u64 words = 3ull * nreg + 8, bytes = words * 4 + 16 * n + 16 * (u64)max_over + 64;
+    void *scratch = nullptr;
+    if (!dev_alloc(&scratch, bytes, s)) return false;
+    u32 *counts = (u32 *)scratch, *cursor = counts + nreg, *offsets = cursor + nreg;
+    ulonglong2 *tmp = (ulonglong2 *)(((uintptr_t)(offsets + nreg + 2) + 15) & ~(uintptr_t)15);
+    ulonglong2 *over = tmp + n;
+    bool ok = CGB_CUDA(cudaMemsetAsync(counts, 0, 2ull * nreg * 4, s)) &&
+              CGB_CUDA(cudaMemsetAsync(c.d + 6, 0, sizeof(u64), s)) && CGB_CUDA(cudaMemsetAsync(c.err, 0, 4, s));
+    u32 *n_over = (u32 *)(c.d + 6);
+    if (ok) {
+        kclock().begin(s, &kstats().index_ms);
+        const int grid = grid_for(n, 256, 8);
+        region_count_kernel<<<grid, 256, 0, s>>>(ix.keys, n, cap, counts);
+        region_scan_kernel<<<1, 1024, 0, s>>>(counts, nreg, offsets);
+        if (vbytes == 8)
+            region_scatter_kernel<double><<<grid, 256, 0, s>>>(ix.keys, (const double *)ix.vals, n, cap, offsets,
+                                                                cursor, tmp);
+        else
+            region_scatter_kernel<float><<<grid, 256, 0, s>>>(ix.keys, (const float *)ix.vals, n, cap, offsets,
+                                                               cursor, tmp);
+        region_build_kernel<<<std::min<u32>(nreg, (u32)NUM_SMS_B200 * 4), 512, 0, s>>>(
+            tmp, offsets, nreg, cap, (ulonglong2 *)st.p, over, max_over, n_over, c.err);
+        kclock().end(s);
+        kstats().launches += 3;
+        ok = CGB_CUDA(cudaGetLastError());
+    }
+    u32 h[2] = {0, 0};  // overflow count, error word
+    ok = ok && CGB_CUDA(cudaMemcpyAsync(&h[0], n_over, 4, cudaMemcpyDeviceToHost, s)) &&
+         CGB_CUDA(cudaMemcpyAsync(&h[1], c.err, 4, cudaMemcpyDeviceToHost, s)) && CGB_CUDA(cudaStreamSynchronize(s));
+    kclock().flush();
+    if (ok && h[1] == 0 && h[0]) {
+        kclock().begin(s, &kstats().index_ms);
+        overflow_insert_kernel<<<std::max<u32>(1, std::min<u32>((h[0] + 255) / 256, 1024)), 256, 0, s>>>(
+            over, h[0], (ulonglong2 *)st.p, cap, c.err);
+        kclock().end(s);
+        kstats().launches++;
+        ok = CGB_CUDA(cudaGetLastError()) && CGB_CUDA(cudaMemcpyAsync(&h[1], c.err, 4, cudaMemcpyDeviceToHost, s)) &&
+             CGB_CUDA(cudaStreamSynchronize(s));
+        kclock().flush();
+    }
+    dev_free(scratch, s);
+    if (!ok) return false;
+    if (h[1]) return true;  // the overflow list ran out: the atomic build instead
+    ix.kind = INDEX_HASH;
+    ix.slots = st.p;
+    ix.cap = cap;
+    kstats().index_builds++;
+    return true;
+}
+
 bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
                  cudaStream_t s)
 {
@@ -592,6 +752,10 @@ bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int buc
     ix.ch = CompactHash{};
     if (kind == INDEX_HASH && vbytes == 4 && g_hash_compact && ix.n >= 64) {
         if (!build_compact(ix, st, c, s)) return false;
+        if (ix.kind == INDEX_HASH) return true;
+    }
+    if (kind == INDEX_HASH && g_region_build && ix.n >= (1u << 16) && ix.n <= (1u << 28)) {
+        if (!build_regions(ix, vbytes, st, c, s)) return false;
         if (ix.kind == INDEX_HASH) return true;
     }
     if (kind == INDEX_HASH) {

@@ -42,6 +42,7 @@ extern int g_solve_variant;
 extern int g_sort_variant;
 extern int g_hash_load_pct;
 extern int g_hash_compact;
+extern int g_region_build;
 }
 
 static Engine &E() { return Engine::get(); }
@@ -162,6 +163,12 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         g_dev_mem_cap = (u64)value << 20;
+    } else if (k == "region_build") {
+        if (value < 0 || value > 1) {
+            set_error("cgb_set_option: region_build must be 0 or 1");
+            return -1;
+        }
+        g_region_build = (int)value;
     } else if (k == "hash_compact") {
         if (value < 0 || value > 1) {
             set_error("cgb_set_option: hash_compact must be 0 or 1");
@@ -201,6 +208,7 @@ long long cgb_get_option(const char *name)
     if (k == "host_layers_mb") return (long long)(E().host_layers_cap >> 20);
     if (k == "fp64_top_layers") return E().fp64_top_layers;
     if (k == "hash_compact") return g_hash_compact;
+    if (k == "region_build") return g_region_build;
     if (k == "lookback_spin_limit") return g_test_spin;
     if (k == "lookback_hold_first_tile") return g_test_hold;
     if (k == "device_mem_cap_mb") return (long long)(g_dev_mem_cap >> 20);

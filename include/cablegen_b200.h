@@ -49,6 +49,9 @@ int cgb_set_rules(const cgb_rules *rules);
  * second copy; default 65536),
  * "hash_load_pct" (target load factor of the hash index, 10..90, or 0, the
  * default: 25 up to 2^27 keys per table, 45 above),
+ * "region_build" (1, the default: 16-byte-slot hash indexes of 2^16..2^28 keys
+ * built region by region in shared memory; 0: atomic inserts into a zeroed table),
+ * "hash_compact" (1, the default: FP32 tables in 8-byte slots where the keys allow),
  * "fp64_top_layers" (FP32 sweeps of cgb_sweep_run: the highest layers, solved
  * first, whose values come straight from the winstates, are solved in FP64 and
  * narrowed to FP32 for the layers below; default 4, 0 = none).

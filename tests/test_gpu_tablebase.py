@@ -123,6 +123,26 @@ def test_solve_variants_agree(cuda, precision, name, end):
             assert sha_table(k, vals) == rec["tables_sha256"], s
 
 
+def test_region_built_index_matches_atomic_build(cuda):
+    """The 16-byte-slot index built region by region in shared memory (layers of 2^16..2^28
+    keys) answers exactly like the one built by atomic inserts: FP64 tables bit-equal."""
+    w = configs.get("ll_pruned", end_gen=220)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    old = cuda.get_option("region_build")
+    got = {}
+    try:
+        for v in (0, 1):
+            cuda.set_option("region_build", v)
+            _, got[v], _ = cuda.tablebase(f.initial, f.start, f.end_gen, f.start, f.winstates, precision=64,
+                                          keep_tables=True)
+    finally:
+        cuda.set_option("region_build", old)
+    assert max(len(k) for k, _ in got[1].values()) >= (1 << 16)
+    for s in got[0]:
+        assert np.array_equal(got[0][s][1], got[1][s][1]), s
+
+
 def test_fp32_compact_index_matches_wide(cuda):
     """FP32 tables looked up through 8-byte slots equal those through 16-byte slots, bit for
     bit (both indexes are exact), and the large layers of LL do take the 8-byte form."""
