@@ -387,6 +387,13 @@ def run_ours(args):
     dev_ms = sum(s["total_ms"] for s in stats)
     boards = sum(s["boards_generated"] + s["boards_solved"] for s in stats)
     gpu_launches = kst["launches"]
+    # per phase, per step: the sweep's device time and the part its kernels take (the rest is
+    # copies, memsets, allocation and the gaps of host round trips)
+    k = max(args.steps, 1)
+    gen_k = sum(kst[f"{f}_ms"] for f in ("expand", "spawn", "onesweep", "hist", "unique", "merge"))
+    sol_k = kst["solve_ms"] + kst["index_ms"]
+    phases = {"gen_ms": sum(s["gen_ms"] for s in stats) / k, "gen_kernel_ms": gen_k / k,
+              "solve_ms": sum(s["solve_ms"] for s in stats) / k, "solve_kernel_ms": sol_k / k}
 
     # ---- FP32 sweep, its error against FP64, and the plain (bisection) FP64 solve
     fp32 = None
@@ -595,6 +602,7 @@ def run_ours(args):
                 "data": "synthetic (seeded SplitMix64 initial boards)",
                 "config": bench_config(args.workload, args.end),
                 "parallelism": f"replicas x{world}", "boards_per_step": boards // max(args.steps, 1),
+                "phases": phases,
                 "wall_s": wall, "gpu_launches": gpu_launches, "clocks": clock_summary, "roofline": roofline,
                 "fp32": fp32, "precision": precision, "e2e": e2e, "like_for_like": like, "large": large,
                 "batch": batch,

@@ -12,7 +12,7 @@ namespace cgb {
 
 // ---- sort / unique / merge (sort.cu) ------------------------------------
 struct SortWorkspace {
-    static constexpr int SMALL_WORDS = 4096;
+    static constexpr int SMALL_WORDS = 8192;
     u32 *small = nullptr;       // histograms, tile counters, error word, counts
     u32 *lookback = nullptr;    // decoupled look-back state
     u64 lookback_bytes = 0;

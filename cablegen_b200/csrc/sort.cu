@@ -136,6 +136,17 @@ __global__ void __launch_bounds__(256) digit_histogram_kernel(const u64 *__restr
     }
 }
 
+// the exclusive prefix of each digit's histogram (block d scans digit d): the
+// global start of every bin, read by the byte-digit passes instead of a block
+// scan per tile
+__global__ void __launch_bounds__(RADIX) digit_offsets_kernel(const u32 *__restrict__ hist, u32 *__restrict__ offs)
+{
+    __shared__ u32 scratch[33];
+    u32 total;
+    offs[blockIdx.x * RADIX + threadIdx.x] =
+        block_exclusive_scan<u32>(hist[blockIdx.x * RADIX + threadIdx.x], scratch, &total);
+}
+
 // ---------------------------------------------------------------------------
 // one digit pass: src -> dst, stable by the digit at `shift`
 __global__ void __launch_bounds__(SORT_THREADS) onesweep_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst,
@@ -369,7 +380,7 @@ struct BytePassSmem {
 
 template <int THREADS, bool FULL>
 __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
-                                               const u32 *__restrict__ digit_hist, u32 *lookback, u32 tile, u32 *err,
+                                               const u32 *__restrict__ bin_base, u32 *lookback, u32 tile, u32 *err,
                                                BytePassSmem<THREADS> &S)
 {
     constexpr u32 TILE = (u32)BytePassSmem<THREADS>::TILE;
@@ -449,8 +460,8 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
         excl = lookback_sum(lookback + d, RADIX, (int)tile - 1, err);
         st_relaxed(lookback + (u64)tile * RADIX + d, LB_PRE | (excl + cnt));
     }
-    const u32 gexcl = block_exclusive_scan<u32>(d < RADIX ? digit_hist[d] : 0u, S.scan, &total);
-    if (d < RADIX) S.bin_delta[d] = gexcl + excl - lstart;
+    // bin_base: the digit's exclusive prefix over all keys, scanned once per pass
+    if (d < RADIX) S.bin_delta[d] = bin_base[d] + excl - lstart;
     __syncthreads();
     const bool hiw = shift >= 32;
     const u32 tile_n = FULL ? TILE : min(TILE, n - tile_base);
@@ -467,7 +478,7 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 5 : 2)
     onesweep_byte_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
-                         const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err)
+                         const u32 *__restrict__ bin_base, u32 *lookback, u32 *tile_counter, u32 *err)
 {
     extern __shared__ __align__(16) unsigned char byte_smem[];
     BytePassSmem<THREADS> &S = *reinterpret_cast<BytePassSmem<THREADS> *>(byte_smem);
@@ -476,9 +487,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 5 : 2)
     __syncthreads();
     const u32 tile = S.tile;
     if ((u64)(tile + 1) * BytePassSmem<THREADS>::TILE <= n)
-        byte_pass_tile<THREADS, true>(src, dst, n, shift, digit_hist, lookback, tile, err, S);
+        byte_pass_tile<THREADS, true>(src, dst, n, shift, bin_base, lookback, tile, err, S);
     else
-        byte_pass_tile<THREADS, false>(src, dst, n, shift, digit_hist, lookback, tile, err, S);
+        byte_pass_tile<THREADS, false>(src, dst, n, shift, bin_base, lookback, tile, err, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -938,7 +949,7 @@ void SortWorkspace::release(cudaStream_t s)
 
 // small words: [0,2048) histograms, [2048,2064) tile counters, 2064 err, 2065 count,
 // 2066-2067 a 64-bit count (8-byte aligned)
-static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065, W_COUNT64 = 2066;
+static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065, W_COUNT64 = 2066, W_OFFS = 4096;
 
 static bool check_err(SortWorkspace &ws, cudaStream_t s, const char *what)
 {
@@ -993,6 +1004,11 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     kstats().hist_bytes += 8 * n;
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u32 hist[8 * RADIX];
+    if (g_sort_variant == 3 || g_sort_variant == 4) {
+        digit_offsets_kernel<<<8, RADIX, 0, s>>>(ws.small + W_HIST, ws.small + W_OFFS);
+        kstats().launches++;
+        if (!CGB_CUDA(cudaGetLastError())) return false;
+    }
     if (!CGB_CUDA(cudaMemcpyAsync(hist, ws.small + W_HIST, sizeof(hist), cudaMemcpyDeviceToHost, s))) return false;
     if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     int digits[8];
@@ -1027,11 +1043,11 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
                                                                   ws.small + W_CTR + p, ws.small + W_ERR);
         else if (variant == 3)
             onesweep_byte_kernel<256><<<ceil_div(n, 256 * BAL_KPT), 256, sizeof(BytePassSmem<256>), s>>>(
-                src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX, ws.lookback, ws.small + W_CTR + p,
+                src, dst, (u32)n, 8 * d, ws.small + W_OFFS + d * RADIX, ws.lookback, ws.small + W_CTR + p,
                 ws.small + W_ERR);
         else if (variant == 4)
             onesweep_byte_kernel<512><<<ceil_div(n, 512 * BAL_KPT), 512, sizeof(BytePassSmem<512>), s>>>(
-                src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX, ws.lookback, ws.small + W_CTR + p,
+                src, dst, (u32)n, 8 * d, ws.small + W_OFFS + d * RADIX, ws.lookback, ws.small + W_CTR + p,
                 ws.small + W_ERR);
         else
             onesweep_kernel<<<tiles, SORT_THREADS, 0, s>>>(src, dst, (u32)n, 8 * d, ws.small + W_HIST + d * RADIX,
