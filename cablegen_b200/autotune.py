@@ -7,7 +7,7 @@ The knobs (cgb_set_option):
   persistent CTAs that bulk-copy the next tile into shared memory while ranking the current one,
   3 is the ballot pass specialised for byte digits (full tiles without bounds tests, digits read
   from the one 32-bit word that holds them), 4 the same with 8192-key tiles of 512 threads (the
-  tile-size knob);
+  tile-size knob), 5 is 4 ranking each key with one warp match in place of eight ballots;
 * ``solve_variant`` -- 0 one thread per board, 1 the (board, empty cell) pairs of 32 boards
   spread over a warp;
 * ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
@@ -31,7 +31,7 @@ from typing import Dict, Optional
 from . import configs, device
 
 KNOBS = {
-    "sort_variant": [4, 3, 1, 0, 2],
+    "sort_variant": [4, 5, 3, 1, 0, 2],
     "solve_variant": [1, 0],
     "hash_load_pct": [0, 25, 45],
 }

@@ -35,7 +35,7 @@ constexpr int UNQ_KPT = 16;
 constexpr int UNQ_TILE = UNQ_THREADS * UNQ_KPT;
 
 constexpr int MRG_THREADS = 256;
-constexpr int MRG_KPT = 8;
+constexpr int MRG_KPT = 16;
 constexpr int MRG_TILE = MRG_THREADS * MRG_KPT;
 
 // Walk back over the look-back words of one bin (or of the whole tile),
@@ -79,6 +79,65 @@ __device__ __forceinline__ u32 lookback_sum(const u32 *words, u64 stride, int j,
         if (stalled) {
             if (++spins > limit) {
                 atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    return excl;
+}
+
+__device__ __forceinline__ u64 ld_relaxed64(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(u64 *p, u64 v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Warp-wide form of the walk back over one count per tile, called by all 32
+// lanes of one warp: lane i reads the word of tile j - i, so one round trip
+// covers 32 predecessors.  The words from tile j down to the nearest inclusive
+// prefix (or down to the first one not yet published, which is polled again)
+// are summed with a warp reduction.  Every lane returns the same prefix.
+template <typename W>
+__device__ __forceinline__ W warp_lookback_sum(const W *words, int j, u32 *err)
+{
+    constexpr W PRE = (W)2 << (8 * sizeof(W) - 2);
+    constexpr W MASK = ((W)1 << (8 * sizeof(W) - 2)) - 1;
+    const int lane = threadIdx.x & 31;
+    W excl = 0;
+    u32 spins = 0;
+    const u32 limit = g_spin_limit;
+    while (j >= 0) {
+        const int k = j - lane;
+        W v;
+        if (k >= 0) {
+            if constexpr (sizeof(W) == 8) v = ld_relaxed64((const u64 *)words + k);
+            else v = ld_relaxed((const u32 *)words + k);
+        } else {
+            v = PRE;  // before tile 0: an empty inclusive prefix ends the walk
+        }
+        const W flag = v & ~MASK;
+        const u32 pre = __ballot_sync(0xffffffffu, flag == PRE);
+        const u32 unready = __ballot_sync(0xffffffffu, flag == 0);
+        // lanes that count: up to the nearest inclusive prefix, and short of
+        // the first word not yet published
+        const u32 upto = pre ? ((pre & (0u - pre)) << 1) - 1 : 0xffffffffu;
+        const u32 stop = unready & upto;
+        const u32 take = stop ? (stop & (0u - stop)) - 1 : upto;
+        W c = ((take >> lane) & 1) ? (v & MASK) : (W)0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        excl += c;
+        if (!stop && pre) break;
+        j -= __popc(take);
+        if (stop) {
+            if (++spins > limit) {
+                if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 break;
             }
             __nanosleep(32);
@@ -378,7 +437,7 @@ struct BytePassSmem {
     u32 tile;
 };
 
-template <int THREADS, bool FULL>
+template <int THREADS, bool FULL, bool MATCH>
 __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
                                                const u32 *__restrict__ bin_base, u32 *lookback, u32 tile, u32 *err,
                                                BytePassSmem<THREADS> &S)
@@ -409,10 +468,17 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
             const u32 idx = warp_base + i * 32 + lane;
             peers = __ballot_sync(0xffffffffu, idx < n);
         }
+        if (MATCH) {
+            // one match instruction in place of eight ballots; a lane past the
+            // end matches only itself
+            const u32 idx = warp_base + i * 32 + lane;
+            peers &= __match_any_sync(0xffffffffu, (FULL || idx < n) ? d : RADIX + lane);
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const u32 bj = __ballot_sync(0xffffffffu, (d >> j) & 1);
-            peers &= ((d >> j) & 1) ? bj : ~bj;
+            for (int j = 0; j < 8; j++) {
+                const u32 bj = __ballot_sync(0xffffffffu, (d >> j) & 1);
+                peers &= ((d >> j) & 1) ? bj : ~bj;
+            }
         }
         const u32 base = S.warp_hist[warp][d];   // every peer reads the same word
         __syncwarp();
@@ -475,7 +541,7 @@ __device__ __forceinline__ void byte_pass_tile(const u64 *__restrict__ src, u64 
     }
 }
 
-template <int THREADS>
+template <int THREADS, bool MATCH = false>
 __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 5 : 2)
     onesweep_byte_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
                          const u32 *__restrict__ bin_base, u32 *lookback, u32 *tile_counter, u32 *err)
@@ -487,9 +553,9 @@ __global__ void __launch_bounds__(THREADS, THREADS == 256 ? 5 : 2)
     __syncthreads();
     const u32 tile = S.tile;
     if ((u64)(tile + 1) * BytePassSmem<THREADS>::TILE <= n)
-        byte_pass_tile<THREADS, true>(src, dst, n, shift, bin_base, lookback, tile, err, S);
+        byte_pass_tile<THREADS, true, MATCH>(src, dst, n, shift, bin_base, lookback, tile, err, S);
     else
-        byte_pass_tile<THREADS, false>(src, dst, n, shift, bin_base, lookback, tile, err, S);
+        byte_pass_tile<THREADS, false, MATCH>(src, dst, n, shift, bin_base, lookback, tile, err, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -661,7 +727,7 @@ static int pipe_grid(int device)
 
 // 0: match ranking, 1: ballot ranking, 2: pipelined persistent, 3: byte-digit ballot
 // (4096-key tiles), 4: byte-digit ballot with 8192-key tiles (the default: measured
-// 9 % faster than 3 on the LL sweep)
+// 9 % faster than 3 on the LL sweep), 5: 4 with match ranking
 int g_sort_variant = 4;
 
 // the 8192-key byte pass needs more than the default 48 KiB of shared memory
@@ -669,8 +735,10 @@ static bool byte512_attr()
 {
     static bool done = false;
     if (!done) {
-        if (!CGB_CUDA(cudaFuncSetAttribute(onesweep_byte_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sizeof(BytePassSmem<512>))))
+        if (!CGB_CUDA(cudaFuncSetAttribute(onesweep_byte_kernel<512, false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BytePassSmem<512>))) ||
+            !CGB_CUDA(cudaFuncSetAttribute(onesweep_byte_kernel<512, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BytePassSmem<512>))))
             return false;
         done = true;
     }
@@ -687,60 +755,99 @@ bool set_lookback_test(u32 spin_limit, int hold_first_tile)
 }
 
 // ---------------------------------------------------------------------------
-// padded shared-memory index for blocked reads of 16 consecutive u64
-__device__ __forceinline__ u32 pad16(u32 j) { return j + (j >> 4); }
-
-// unique: in (sorted) -> out, dropping repeats; *out_count = number kept
-__global__ void __launch_bounds__(UNQ_THREADS) unique_kernel(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out,
-                                                             u32 *lookback, u32 *tile_counter, u32 *out_count,
-                                                             u32 *err)
+// 8-byte global -> shared copies that hold no registers while in flight
+__device__ __forceinline__ void cp_async8(void *dst_smem, const void *src_gmem)
 {
-    __shared__ u64 keys_sh[UNQ_TILE + UNQ_TILE / 16];
-    __shared__ u32 scan_scratch[33];
-    __shared__ u32 tile_sh, prefix_sh;
-    if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const u32 tile = tile_sh;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst_smem)), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// unique: in (sorted) -> out, dropping repeats; *out_count = number kept.
+// The tile (and the key before it) is staged in shared memory by async
+// copies, all of a thread's in flight at once and no registers held.  Warp w
+// then owns keys [512w, 512w + 512) as 16 rows of 32: a key's predecessor is
+// the shared word before it, the kept keys of a row are ranked with one
+// ballot, and each row's kept keys go out as one coalesced store.  Warp 0
+// scans the eight warp totals and runs the tile's look-back.
+struct UniqueSmem {
+    u64 keys[UNQ_TILE + 1];  // keys[0]: the key before the tile
+    u32 warp_base[UNQ_THREADS / 32];
+    u32 tile;
+};
+
+template <bool FULL>
+__device__ __forceinline__ void unique_tile(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out, u32 *lookback,
+                                            u32 tile, u32 *out_count, u32 *err, UniqueSmem &S)
+{
+    constexpr u32 ALL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const u32 tile_base = tile * UNQ_TILE;
-    const u32 tile_n = min((u32)UNQ_TILE, n - tile_base);
-    for (u32 j = threadIdx.x; j < tile_n; j += UNQ_THREADS) keys_sh[pad16(j)] = in[tile_base + j];
-    __syncthreads();
-    const u64 before = tile_base ? in[tile_base - 1] : 0;
-    // thread t owns keys [16t, 16t+16) of the tile
-    u32 flags = 0;
-    u64 prev = (threadIdx.x == 0) ? before : 0;
-    if (threadIdx.x > 0 && 16 * threadIdx.x <= tile_n) prev = keys_sh[pad16(16 * threadIdx.x - 1)];
+    const u32 tile_n = FULL ? (u32)UNQ_TILE : n - tile_base;
 #pragma unroll
-    for (int i = 0; i < UNQ_KPT; i++) {
-        const u32 j = 16 * threadIdx.x + i;
-        if (j < tile_n) {
-            const u64 v = keys_sh[pad16(j)];
-            const bool first = (tile_base + j == 0) || v != prev;
-            if (first) flags |= 1u << i;
-            if (tile_base + j > 0 && v < prev) atomicOr(err, ERR_UNSORTED);
-            prev = v;
+    for (int q = 0; q < UNQ_KPT; q++) {
+        const u32 j = q * UNQ_THREADS + threadIdx.x;
+        if (FULL || j < tile_n) cp_async8(&S.keys[1 + j], in + tile_base + j);
+    }
+    if (threadIdx.x == 0 && tile_base > 0) cp_async8(&S.keys[0], in + tile_base - 1);
+    cp_async_wait_all();
+    __syncthreads();
+    const u32 wfirst = warp * (UNQ_KPT * 32);
+    u32 mask[UNQ_KPT];
+    u32 total = 0;
+    bool descent = false;
+#pragma unroll
+    for (int q = 0; q < UNQ_KPT; q++) {
+        const u32 j = wfirst + q * 32 + lane;
+        const bool valid = FULL || j < tile_n;
+        const bool has_prev = tile_base + j > 0;
+        const u64 v = valid ? S.keys[1 + j] : 0ull;
+        const u64 prev = (valid && has_prev) ? S.keys[j] : 0ull;
+        descent |= valid && has_prev && v < prev;
+        mask[q] = __ballot_sync(ALL, valid && (!has_prev || v != prev));
+        total += __popc(mask[q]);
+    }
+    if (descent) atomicOr(err, ERR_UNSORTED);
+    if (lane == 0) S.warp_base[warp] = total;
+    __syncthreads();
+    if (warp == 0) {
+        const u32 c = lane < UNQ_THREADS / 32 ? S.warp_base[lane] : 0u;
+        const u32 incl = warp_inclusive_scan(c);
+        const u32 tile_total = __shfl_sync(ALL, incl, 31);
+        u32 prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) st_relaxed(lookback, LB_PRE | tile_total);
+        } else {
+            if (lane == 0) st_relaxed(lookback + tile, LB_AGG | tile_total);
+            prefix = warp_lookback_sum<u32>(lookback, (int)tile - 1, err);
+            if (lane == 0) st_relaxed(lookback + tile, LB_PRE | (prefix + tile_total));
         }
+        if (lane < UNQ_THREADS / 32) S.warp_base[lane] = prefix + incl - c;
+        if (lane == 0 && tile_base + UNQ_TILE >= n) *out_count = prefix + tile_total;
     }
-    const u32 cnt = __popc(flags);
-    u32 tile_total;
-    const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &tile_total);
-    // gather the kept keys in place (kept rank <= position, threads ordered)
-    u64 kept[UNQ_KPT];
-#pragma unroll
-    for (int i = 0; i < UNQ_KPT; i++) kept[i] = keys_sh[pad16(16 * threadIdx.x + i)];
     __syncthreads();
-    u32 w = excl;
+    u32 pos = S.warp_base[warp];
+    const u32 lt = lanemask_lt();
 #pragma unroll
-    for (int i = 0; i < UNQ_KPT; i++)
-        if (flags & (1u << i)) keys_sh[pad16(w++)] = kept[i];
-    if (threadIdx.x == 0) prefix_sh = tile_lookback(lookback, tile, tile_total, err);
-    __syncthreads();
-    const u32 prefix = prefix_sh;
-    for (u32 j = threadIdx.x; j < tile_total; j += UNQ_THREADS) {
-        if (prefix + j < n) out[prefix + j] = keys_sh[pad16(j)];
-        else atomicOr(err, ERR_CAPACITY);
+    for (int q = 0; q < UNQ_KPT; q++) {
+        if ((mask[q] >> lane) & 1) {
+            const u32 g = pos + __popc(mask[q] & lt);
+            if (g < n) out[g] = S.keys[1 + wfirst + q * 32 + lane];
+            else atomicOr(err, ERR_CAPACITY);
+        }
+        pos += __popc(mask[q]);
     }
-    if (threadIdx.x == 0 && tile_base + UNQ_TILE >= n) *out_count = prefix + tile_total;
+}
+
+__global__ void __launch_bounds__(UNQ_THREADS, 5) unique_kernel(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out,
+                                                                u32 *lookback, u32 *tile_counter, u32 *out_count,
+                                                                u32 *err)
+{
+    __shared__ UniqueSmem S;
+    if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const u32 tile = S.tile;
+    if ((u64)(tile + 1) * UNQ_TILE <= n) unique_tile<true>(in, n, out, lookback, tile, out_count, err, S);
+    else unique_tile<false>(in, n, out, lookback, tile, out_count, err, S);
 }
 
 // ---------------------------------------------------------------------------
@@ -762,16 +869,6 @@ __device__ __forceinline__ u32 merge_path(const u64 *a, u32 na, const u64 *b, u3
 // positions and a 64-bit look-back word (2 flag bits, 62-bit count)
 constexpr u64 LB64_AGG = 1ull << 62, LB64_PRE = 2ull << 62, LB64_MASK = (1ull << 62) - 1;
 
-__device__ __forceinline__ u64 ld_relaxed64(const u64 *p)
-{
-    u64 v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed64(u64 *p, u64 v)
-{
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
 
 __device__ __forceinline__ u64 tile_lookback64(u64 *lookback, u32 tile, u64 count, u32 *err)
 {
@@ -823,18 +920,25 @@ __global__ void merge_partition_kernel(const u64 *__restrict__ a, u64 na, const 
     splits[t] = merge_path64(a, na, b, nb, diag);
 }
 
+// One tile of MRG_TILE merged positions: the tile's runs of a and b are loaded
+// with all of a thread's loads in flight, each thread merges MRG_KPT positions
+// from its merge-path split (the heads of both runs held in registers), marks
+// the first of each run of equal keys, and the kept keys are staged in the
+// same shared buffer (the runs are no longer read by then) for one coalesced
+// write.  Warp 0 scans the warp totals and runs the 64-bit look-back.
 __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__restrict__ a, u64 na,
                                                                    const u64 *__restrict__ b, u64 nb,
                                                                    const u64 *__restrict__ splits,
                                                                    u64 *__restrict__ out, u64 *lookback,
                                                                    u32 *tile_counter, u64 *out_count, u32 *err)
 {
-    __shared__ u64 in_sh[MRG_TILE];
-    __shared__ u64 out_sh[MRG_TILE + MRG_TILE / 8];
-    __shared__ u32 scan_scratch[33];
+    constexpr u32 ALL = 0xffffffffu;
+    __shared__ u64 buf[MRG_TILE + MRG_TILE / 8];
     __shared__ u64 last_sh[MRG_THREADS];
-    __shared__ u32 tile_sh;
+    __shared__ u32 warp_sh[MRG_THREADS / 32];
+    __shared__ u32 tile_sh, kept_sh;
     __shared__ u64 prefix_sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) tile_sh = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const u32 tile = tile_sh;
@@ -844,29 +948,51 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
     const u64 a0 = splits[tile], a1 = splits[tile + 1];
     const u64 b0 = d0 - a0, b1 = d1 - a1;
     const u32 la = (u32)(a1 - a0), lb = (u32)(b1 - b0);
-    for (u32 j = threadIdx.x; j < la; j += MRG_THREADS) in_sh[j] = a[a0 + j];
-    for (u32 j = threadIdx.x; j < lb; j += MRG_THREADS) in_sh[la + j] = b[b0 + j];
-    __syncthreads();
-    const u64 *sa = in_sh, *sb = in_sh + la;
+    {
+        u64 r[MRG_KPT];
+#pragma unroll
+        for (int i = 0; i < MRG_KPT; i++) {
+            const u32 j = i * MRG_THREADS + threadIdx.x;
+            r[i] = j < la ? a[a0 + j] : (j < la + lb ? b[b0 + (j - la)] : 0ull);
+        }
+#pragma unroll
+        for (int i = 0; i < MRG_KPT; i++) {
+            const u32 j = i * MRG_THREADS + threadIdx.x;
+            if (j < la + lb) buf[j] = r[i];
+        }
+    }
     // the merged element just before this tile
     const bool have_before = d0 > 0;
     u64 before = 0;
-    if (have_before) {
+    if (have_before && threadIdx.x == 0) {
         if (a0 == 0) before = b[b0 - 1];
         else if (b0 == 0) before = a[a0 - 1];
         else before = max(a[a0 - 1], b[b0 - 1]);
     }
+    __syncthreads();
+    const u64 *sa = buf, *sb = buf + la;
     const u32 len = (u32)(d1 - d0);
     const u32 t0 = min((u32)(threadIdx.x * MRG_KPT), len);
     const u32 t1 = min(t0 + MRG_KPT, len);
     u32 ia = merge_path(sa, la, sb, lb, t0);
     u32 ib = t0 - ia;
+    u64 xa = ia < la ? sa[ia] : 0ull, xb = ib < lb ? sb[ib] : 0ull;
     u64 v[MRG_KPT];
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++) {
         if (t0 + i < t1) {
-            const bool take_a = ib >= lb || (ia < la && sa[ia] <= sb[ib]);
-            v[i] = take_a ? sa[ia++] : sb[ib++];
+            const bool take_a = ib >= lb || (ia < la && xa <= xb);
+            if (take_a) {
+                v[i] = xa;
+                ++ia;
+                xa = ia < la ? sa[ia] : 0ull;
+            } else {
+                v[i] = xb;
+                ++ib;
+                xb = ib < lb ? sb[ib] : 0ull;
+            }
+        } else {
+            v[i] = 0ull;
         }
     }
     u64 mylast = 0;
@@ -874,7 +1000,7 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
     for (int i = 0; i < MRG_KPT; i++)
         if (t0 + i < t1) mylast = v[i];
     last_sh[threadIdx.x] = mylast;
-    __syncthreads();
+    __syncthreads();  // after this the runs in buf are no longer read
     u64 prev;
     bool have_prev;
     if (threadIdx.x == 0) {
@@ -898,23 +1024,43 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
     }
     if (descent) atomicOr(err, ERR_UNSORTED);
     const u32 cnt = __popc(flags);
-    u32 tile_total;
-    const u32 excl = block_exclusive_scan<u32>(cnt, scan_scratch, &tile_total);
-    u32 w = excl;
+    const u32 inc = warp_inclusive_scan(cnt);
+    if (lane == 31) warp_sh[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const u32 c = lane < MRG_THREADS / 32 ? warp_sh[lane] : 0u;
+        const u32 wi = warp_inclusive_scan(c);
+        const u32 tile_total = __shfl_sync(ALL, wi, 31);
+        u64 prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) st_relaxed64(lookback, LB64_PRE | tile_total);
+        } else {
+            if (lane == 0) st_relaxed64(lookback + tile, LB64_AGG | tile_total);
+            prefix = warp_lookback_sum<u64>(lookback, (int)tile - 1, err);
+            if (lane == 0) st_relaxed64(lookback + tile, LB64_PRE | (prefix + tile_total));
+        }
+        if (lane < MRG_THREADS / 32) warp_sh[lane] = wi - c;
+        if (lane == 0) {
+            prefix_sh = prefix;
+            kept_sh = tile_total;
+            if ((u64)(tile + 1) * MRG_TILE >= total) *out_count = prefix + tile_total;
+        }
+    }
+    __syncthreads();
+    u32 w = warp_sh[warp] + inc - cnt;
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++)
         if (flags & (1u << i)) {
-            out_sh[w + (w >> 3)] = v[i];
+            buf[w + (w >> 3)] = v[i];
             w++;
         }
-    if (threadIdx.x == 0) prefix_sh = tile_lookback64(lookback, tile, tile_total, err);
     __syncthreads();
     const u64 prefix = prefix_sh;
-    for (u32 j = threadIdx.x; j < tile_total; j += MRG_THREADS) {
-        if (prefix + j < total) out[prefix + j] = out_sh[j + (j >> 3)];
+    const u32 kept = kept_sh;
+    for (u32 j = threadIdx.x; j < kept; j += MRG_THREADS) {
+        if (prefix + j < total) out[prefix + j] = buf[j + (j >> 3)];
         else atomicOr(err, ERR_CAPACITY);
     }
-    if (threadIdx.x == 0 && (u64)(tile + 1) * MRG_TILE >= total) *out_count = prefix + tile_total;
 }
 
 // ---------------------------------------------------------------------------
@@ -1004,7 +1150,7 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     kstats().hist_bytes += 8 * n;
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u32 hist[8 * RADIX];
-    if (g_sort_variant == 3 || g_sort_variant == 4) {
+    if (g_sort_variant >= 3) {
         digit_offsets_kernel<<<8, RADIX, 0, s>>>(ws.small + W_HIST, ws.small + W_OFFS);
         kstats().launches++;
         if (!CGB_CUDA(cudaGetLastError())) return false;
@@ -1024,10 +1170,10 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
         if (pgrid <= 0 || (((uintptr_t)keys | (uintptr_t)tmp) & 15)) variant = 1;
     }
     const u32 pass_tiles = variant == 2   ? ceil_div(n, PIPE_TILE)
-                           : variant == 4 ? ceil_div(n, 512 * BAL_KPT)
+                           : variant >= 4 ? ceil_div(n, 512 * BAL_KPT)
                            : (variant == 1 || variant == 3) ? ceil_div(n, BAL_TILE)
                                                             : tiles;
-    if (variant == 4 && !byte512_attr()) return false;
+    if (variant >= 4 && !byte512_attr()) return false;
     u64 *src = keys, *dst = tmp;
     for (int p = 0; p < np; p++) {
         const int d = digits[p];
@@ -1047,6 +1193,10 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
                 ws.small + W_ERR);
         else if (variant == 4)
             onesweep_byte_kernel<512><<<ceil_div(n, 512 * BAL_KPT), 512, sizeof(BytePassSmem<512>), s>>>(
+                src, dst, (u32)n, 8 * d, ws.small + W_OFFS + d * RADIX, ws.lookback, ws.small + W_CTR + p,
+                ws.small + W_ERR);
+        else if (variant == 5)
+            onesweep_byte_kernel<512, true><<<ceil_div(n, 512 * BAL_KPT), 512, sizeof(BytePassSmem<512>), s>>>(
                 src, dst, (u32)n, 8 * d, ws.small + W_OFFS + d * RADIX, ws.lookback, ws.small + W_CTR + p,
                 ws.small + W_ERR);
         else

@@ -108,9 +108,9 @@ int cgb_set_option(const char *name, long long value)
         }
         g_solve_variant = (int)value;
     } else if (k == "sort_variant") {
-        if (value < 0 || value > 4) {
+        if (value < 0 || value > 5) {
             set_error("cgb_set_option: sort_variant must be 0 (match ranking), 1 (ballot ranking), 2 (pipelined), "
-                      "3 (byte-digit ballot ranking) or 4 (byte-digit, 8192-key tiles)");
+                      "3 (byte-digit ballot ranking), 4 (byte-digit, 8192-key tiles) or 5 (4 with match ranking)");
             return -1;
         }
         g_sort_variant = (int)value;

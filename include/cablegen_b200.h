@@ -39,8 +39,10 @@ int cgb_set_rules(const cgb_rules *rules);
  * sorted layer as in lookup(), src/solve.c:108-164; 1 top-bits buckets then
  * bisection; 2 open-addressing hash, the default), "bucket_bits" (buckets of
  * kind 1), "solve_variant" (0 one thread per board, 1 warp-compacted),
- * "sort_variant" (0 match ranking, 1 ballot ranking, the default, 2 persistent
- * CTAs with bulk-copy prefetch of the next tile), "spill_reserve_mb"
+ * "sort_variant" (0 match ranking, 1 ballot ranking, 2 persistent CTAs with
+ * bulk-copy prefetch of the next tile, 3 byte-digit passes over 4096-key tiles,
+ * 4 byte-digit passes over 8192-key tiles, the default, 5 as 4 with one match
+ * instruction per key in place of eight ballots), "spill_reserve_mb"
  * (free device memory kept before resident layers spill to host memory),
  * "max_sort_keys" (larger layer steps are cut into chunks and merged),
  * "store_chunk_mb" (device allocation unit of the resident-layer store),

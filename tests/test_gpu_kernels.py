@@ -42,7 +42,7 @@ def test_expand_spawns(cuda):
 SIZES = [0, 1, 2, 31, 4095, 4096, 4097, 8193, 100_000, 1_000_003, 5_000_001]
 
 
-@pytest.fixture(params=[0, 1, 2, 3, 4], ids=["match", "ballot", "pipelined", "byte", "byte8k"])
+@pytest.fixture(params=[0, 1, 2, 3, 4, 5], ids=["match", "ballot", "pipelined", "byte", "byte8k", "byte8k_match"])
 def sort_variant(cuda, request):
     old = cuda.get_option("sort_variant")
     cuda.set_option("sort_variant", request.param)
@@ -111,5 +111,15 @@ def test_merge_unique(cuda, na, nb):
     b = np.unique(rng.integers(0, 1 << 30, size=nb, dtype=np.uint64))
     if len(a) and len(b):
         b = np.unique(np.concatenate([b, a[::3]]))  # overlap
+    got = cuda.to_numpy(cuda.merge_unique(cuda.to_device(a), cuda.to_device(b)))
+    assert np.array_equal(got, np.union1d(a, b))
+
+
+@pytest.mark.parametrize("na,nb", [(4095, 1), (4096, 4096), (4097, 8191), (3_000_017, 2_000_003)])
+def test_merge_unique_repeats(cuda, na, nb):
+    """Sorted inputs that keep repeats (the spawn streams): the merge drops them."""
+    rng = np.random.default_rng(na + 31 * nb)
+    a = np.sort(rng.integers(0, max(na // 3, 1), size=na, dtype=np.uint64))
+    b = np.sort(rng.integers(0, max(nb // 2, 1), size=nb, dtype=np.uint64) * np.uint64(3))
     got = cuda.to_numpy(cuda.merge_unique(cuda.to_device(a), cuda.to_device(b)))
     assert np.array_equal(got, np.union1d(a, b))

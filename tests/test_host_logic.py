@@ -66,7 +66,7 @@ class FakeDevice:
     def batch(self, forms, precision=32):
         self.runs += 1
         o = self.opts
-        ms = 100 + {3: 8, 4: 9, 1: 10, 0: 5, 2: 0}[o["sort_variant"]] + {0: 7, 1: 0}[o["solve_variant"]] + \
+        ms = 100 + {3: 8, 4: 9, 5: 11, 1: 10, 0: 5, 2: 0}[o["sort_variant"]] + {0: 7, 1: 0}[o["solve_variant"]] + \
             {0: 3, 25: 0, 45: 6}[o["hash_load_pct"]]
         return {}, {}, {"total_ms": float(ms)}
 
