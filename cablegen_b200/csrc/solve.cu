@@ -524,49 +524,58 @@ __global__ void compact_build_kernel(const u64 *__restrict__ keys, const float *
 // partitions the keys by region of their home slot (2048 slots = 32 KiB), builds
 // each region in shared memory and writes it out whole: the table is written
 // once, sequentially, and never zeroed.  A key whose linear probe runs past its
-// region's end goes to an overflow list, inserted afterwards into the finished
-// table with the atomic probe; slots from its home to the region's end are all
-// taken, so the probe order of linear probing is kept.
+// region's end (or whose region's bucket is full) goes to an overflow list,
+// inserted afterwards into the finished table with the atomic probe from its
+// home slot; the slots a placed key skipped were taken when it was placed and
+// stay taken, so every key stays reachable by the linear probe from its home.
 constexpr u32 BUILD_REGION = 2048;
 
-__global__ void region_count_kernel(const u64 *__restrict__ keys, u64 n, u64 cap, u32 *counts)
-{
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
-        atomicAdd(counts + home_slot(keys[i], cap) / BUILD_REGION, 1u);
-}
-
-// exclusive scan of `counts` into `offsets` (nreg + 1 entries), one CTA of 1024 threads
-__global__ void __launch_bounds__(1024) region_scan_kernel(const u32 *counts, u32 nreg, u32 *offsets)
-{
-    __shared__ u32 scratch[33];
-    u32 carry = 0;
-    for (u32 base = 0; base < nreg; base += 1024) {
-        const u32 i = base + threadIdx.x;
-        const u32 v = i < nreg ? counts[i] : 0u;
-        u32 total;
-        const u32 ex = block_exclusive_scan<u32>(v, scratch, &total);
-        if (i < nreg) offsets[i] = carry + ex;
-        carry += total;
-    }
-    if (threadIdx.x == 0) offsets[nreg] = carry;
-}
-
+// Each region owns a bucket of `bcap` pairs in the scratch (the mean count of
+// a region plus eight standard deviations and a margin, so that a bucket runs
+// full almost never); a pair that finds its bucket full joins the overflow
+// list.  Four keys per thread per step keep four cursor atomics in flight.
 template <typename V>
-__global__ void region_scatter_kernel(const u64 *__restrict__ keys, const V *__restrict__ vals, u64 n, u64 cap,
-                                      const u32 *__restrict__ offsets, u32 *cursor, ulonglong2 *tmp)
+__global__ void __launch_bounds__(256) region_scatter_kernel(const u64 *__restrict__ keys, const V *__restrict__ vals,
+                                                             u64 n, u64 cap, u32 bcap, u32 *cursor,
+                                                             ulonglong2 *tmp, ulonglong2 *overflow, u32 max_over,
+                                                             u32 *n_over, u32 *err)
 {
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const u64 key = keys[i];
-        const u32 r = (u32)(home_slot(key, cap) / BUILD_REGION);
-        const u32 p = offsets[r] + atomicAdd(cursor + r, 1u);
-        tmp[p] = make_ulonglong2(key, to_bits<V>(vals[i]));
+    constexpr int U = 4;
+    const u64 stride = (u64)gridDim.x * blockDim.x;
+    for (u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += U * stride) {
+        u64 key[U];
+        V val[U];
+        u32 r[U], p[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const u64 i = i0 + u * stride;
+            key[u] = i < n ? keys[i] : 0ull;
+            val[u] = i < n ? vals[i] : V(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            r[u] = (u32)(home_slot(key[u], cap) / BUILD_REGION);
+            p[u] = i0 + u * stride < n ? atomicAdd(cursor + r[u], 1u) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (i0 + u * stride >= n) continue;
+            const ulonglong2 e = make_ulonglong2(key[u], to_bits<V>(val[u]));
+            if (p[u] < bcap) {
+                tmp[(u64)r[u] * bcap + p[u]] = e;
+            } else {
+                const u32 k = atomicAdd(n_over, 1u);
+                if (k < max_over) overflow[k] = e;
+                else atomicOr(err, ERR_CAPACITY);
+            }
+        }
     }
 }
 
 __global__ void __launch_bounds__(512) region_build_kernel(const ulonglong2 *__restrict__ tmp,
-                                                           const u32 *__restrict__ offsets, u32 nreg, u64 cap,
-                                                           ulonglong2 *slots, ulonglong2 *overflow, u32 max_over,
-                                                           u32 *n_over, u32 *err)
+                                                           const u32 *__restrict__ cursor, u32 bcap, u32 nreg,
+                                                           u64 cap, ulonglong2 *slots, ulonglong2 *overflow,
+                                                           u32 max_over, u32 *n_over, u32 *err)
 {
     __shared__ ulonglong2 tab[BUILD_REGION];
     for (u32 r = blockIdx.x; r < nreg; r += gridDim.x) {
@@ -574,8 +583,10 @@ __global__ void __launch_bounds__(512) region_build_kernel(const ulonglong2 *__r
         __syncthreads();
         const u64 base = (u64)r * BUILD_REGION;
         const u32 len = (u32)min((u64)BUILD_REGION, cap - base);
-        for (u32 j = offsets[r] + threadIdx.x; j < offsets[r + 1]; j += blockDim.x) {
-            const ulonglong2 e = tmp[j];
+        const u32 cnt = min(cursor[r], bcap);
+        const ulonglong2 *bucket = tmp + (u64)r * bcap;
+        for (u32 j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const ulonglong2 e = bucket[j];
             bool placed = false;
             for (u32 sl = (u32)(home_slot(e.x, cap) - base); sl < len; sl++) {
                 if (atomicCAS((unsigned long long *)&tab[sl].x, 0ull, (unsigned long long)e.x) == 0ull) {
@@ -689,32 +700,33 @@ static bool build_regions(LayerIndex &ix, int vbytes, IndexStorage &st, Counters
     const u64 cap = hash_capacity(n);
     const u32 nreg = (u32)((cap + BUILD_REGION - 1) / BUILD_REGION);
     const u32 max_over = (u32)(n / 32 + 4096);
+    // bucket size: the mean pairs of a region plus eight standard deviations and a margin
+    const double mean = (double)n * BUILD_REGION / (double)cap;
+    const u32 bcap = (u32)((mean + 8.0 * sqrt(mean) + 64.0 + 15.0) / 16.0) * 16u;
     if (!ensure_storage(st, cap * 16, s)) return false;
-    // scratch: counts, cursors, offsets (u32), the scattered pairs, the overflow list
-    const u64 words = 3ull * nreg + 8, bytes = words * 4 + 16 * n + 16 * (u64)max_over + 64;
+    // scratch: the cursors (u32), the region buckets, the overflow list
+    const u64 bytes = 4ull * nreg + 64 + 16ull * nreg * bcap + 16ull * max_over;
     void *scratch = nullptr;
     if (!dev_alloc(&scratch, bytes, s)) return false;
-    u32 *counts = (u32 *)scratch, *cursor = counts + nreg, *offsets = cursor + nreg;
-    ulonglong2 *tmp = (ulonglong2 *)(((uintptr_t)(offsets + nreg + 2) + 15) & ~(uintptr_t)15);
-    ulonglong2 *over = tmp + n;
-    bool ok = CGB_CUDA(cudaMemsetAsync(counts, 0, 2ull * nreg * 4, s)) &&
+    u32 *cursor = (u32 *)scratch;
+    ulonglong2 *tmp = (ulonglong2 *)(((uintptr_t)(cursor + nreg) + 15) & ~(uintptr_t)15);
+    ulonglong2 *over = tmp + (u64)nreg * bcap;
+    bool ok = CGB_CUDA(cudaMemsetAsync(cursor, 0, 4ull * nreg, s)) &&
               CGB_CUDA(cudaMemsetAsync(c.d + 6, 0, sizeof(u64), s)) && CGB_CUDA(cudaMemsetAsync(c.err, 0, 4, s));
     u32 *n_over = (u32 *)(c.d + 6);
     if (ok) {
         kclock().begin(s, &kstats().index_ms);
-        const int grid = grid_for(n, 256, 8);
-        region_count_kernel<<<grid, 256, 0, s>>>(ix.keys, n, cap, counts);
-        region_scan_kernel<<<1, 1024, 0, s>>>(counts, nreg, offsets);
+        const int grid = grid_for((n + 3) / 4, 256, 8);
         if (vbytes == 8)
-            region_scatter_kernel<double><<<grid, 256, 0, s>>>(ix.keys, (const double *)ix.vals, n, cap, offsets,
-                                                                cursor, tmp);
+            region_scatter_kernel<double><<<grid, 256, 0, s>>>(ix.keys, (const double *)ix.vals, n, cap, bcap,
+                                                                cursor, tmp, over, max_over, n_over, c.err);
         else
-            region_scatter_kernel<float><<<grid, 256, 0, s>>>(ix.keys, (const float *)ix.vals, n, cap, offsets,
-                                                               cursor, tmp);
+            region_scatter_kernel<float><<<grid, 256, 0, s>>>(ix.keys, (const float *)ix.vals, n, cap, bcap,
+                                                               cursor, tmp, over, max_over, n_over, c.err);
         region_build_kernel<<<std::min<u32>(nreg, (u32)NUM_SMS_B200 * 4), 512, 0, s>>>(
-            tmp, offsets, nreg, cap, (ulonglong2 *)st.p, over, max_over, n_over, c.err);
+            tmp, cursor, bcap, nreg, cap, (ulonglong2 *)st.p, over, max_over, n_over, c.err);
         kclock().end(s);
-        kstats().launches += 3;
+        kstats().launches += 2;
         ok = CGB_CUDA(cudaGetLastError());
     }
     u32 h[2] = {0, 0};  // overflow count, error word
