@@ -12,7 +12,10 @@ The knobs (cgb_set_option):
   spread over a warp;
 * ``hash_load_pct`` -- load factor of the open-addressing index of solved layers (0 picks it by
   table size; a higher load means more probes, a lower one more memory and a lower L2 hit
-  rate).
+  rate);
+* ``move_window`` -- blocks of 1024 consecutive input boards whose moves share one repeat set
+  in the move expansion (more blocks keep fewer repeats out of the sort, at the price of longer
+  probes in a fuller set).
 
 The digit width stays at 8 bits: the look-back words and the per-tile histograms grow with the
 radix (2048 bins at 11 bits), which costs more than the pass it saves on 48 varying key bits.
@@ -34,6 +37,7 @@ KNOBS = {
     "sort_variant": [4, 5, 3, 1, 0, 2],
     "solve_variant": [1, 0],
     "hash_load_pct": [0, 25, 45],
+    "move_window": [1, 2, 4],
 }
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "cablegen_b200", "autotune.json")

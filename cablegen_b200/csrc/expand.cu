@@ -100,28 +100,38 @@ __device__ __forceinline__ void stage_table(unsigned char *smem, const unsigned 
     __syncthreads();
 }
 
-// Set of the move results of one CTA iteration (1024 input boards, at most
-// 4096 results) in shared memory: open addressing over 8192 u64 slots, 0 =
-// empty (no canonical board is 0).  Neighbouring boards of a sorted layer
-// often move to the same board (rows that differ only in where their tiles
-// sit before a slide), so dropping the repeats here keeps about half of the
-// raw move stream out of the sort (measured on LL layers: 1024 consecutive
-// inputs keep 53 % of their results).
+// Set of the move results of one chunk of consecutive input boards (1 to 4
+// CTA iterations of 1024 boards) in shared memory: open addressing over 8192
+// u64 slots, 0 = empty (no canonical board is 0).  Neighbouring boards of a
+// sorted layer often move to the same board (rows that differ only in where
+// their tiles sit before a slide), so dropping the repeats here keeps most of
+// the raw move stream out of the sort.  Measured on LL layers 144-150 (CPU
+// count over the layer's raw moves): a chunk of 1024 boards keeps 51 % of its
+// results, 2048 keep 48 %, 4096 keep 44 % (about 4600 set entries, 56 % of the
+// slots); the whole layer would keep 17 %.
 constexpr int MOVE_SET = 8192;
+// boards (in units of 1024) that share one set, 1..4.  Default 1: on the LL
+// sweep to tile sum 600 a window of 4 kept 10.5 % fewer moves (sort -44 ms
+// per step) but the fuller set's longer probes cost the expansion 108 ms more
+int g_move_window = 1;
 constexpr int PRUNE_BYTES = ((int)sizeof(PruneTable) + 15) / 16 * 16;
 constexpr int EXP_SMEM = TABLE_BYTES + MOVE_SET * 8 + PRUNE_BYTES;
+
+// probes before a key is kept without a slot (a repeat that gets this far is
+// kept too: the sort's unique drops it)
+constexpr u32 MOVE_PROBES = 64;
 
 __device__ __forceinline__ bool set_insert(unsigned long long *set, u64 key)
 {
     u32 h = ((u32)(key >> 32) * 0x9E3779B1u) ^ ((u32)key * 0x85EBCA77u);
     h ^= h >> 15;
-    for (u32 i = 0; i < MOVE_SET; i++) {
+    for (u32 i = 0; i < MOVE_PROBES; i++) {
         const u32 slot = (h + i) & (MOVE_SET - 1);
         const unsigned long long prev = atomicCAS(set + slot, 0ull, (unsigned long long)key);
         if (prev == 0ull) return true;   // first copy
         if (prev == key) return false;   // a repeat
     }
-    return true;  // unreachable: the set is never more than half full
+    return true;
 }
 
 // the four moves of b, pruned, canonicalised (over the plan's images when
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
                                                                       u64 *out_count, const unsigned short *g_move,
                                                                       PruneParams pp, const PruneTable *g_prune,
                                                                       u32 *err, FormationFilter ff, CanonPlan plan,
-                                                                      u64 *raw_count)
+                                                                      u64 *raw_count, u32 window)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ u32 scan_scratch[33];
@@ -167,11 +177,16 @@ __global__ void __launch_bounds__(EXP_THREADS, 1) expand_moves_kernel(const u64 
     stage_table(smem, g_move);
     const RowTable t{(const unsigned short *)smem};
     unsigned long long *set = (unsigned long long *)(smem + TABLE_BYTES);
-    const u64 stride = (u64)gridDim.x * EXP_THREADS;
+    // a CTA takes chunks of `window` x 1024 consecutive boards; the set lives
+    // for one chunk, so repeats among all of a chunk's moves are dropped
+    const u64 chunk = (u64)window * EXP_THREADS;
     u32 raw = 0;  // legal, unpruned moves before the set drops repeats
-    for (u64 first = (u64)blockIdx.x * EXP_THREADS; first < n; first += stride) {
-        for (int i = threadIdx.x; i < MOVE_SET; i += EXP_THREADS) set[i] = 0ull;
-        __syncthreads();
+    for (u64 c0 = (u64)blockIdx.x * chunk; c0 < n; c0 += (u64)gridDim.x * chunk)
+    for (u64 first = c0; first < min(c0 + chunk, n); first += EXP_THREADS) {
+        if (first == c0) {
+            for (int i = threadIdx.x; i < MOVE_SET; i += EXP_THREADS) set[i] = 0ull;
+            __syncthreads();
+        }
         const u64 idx = first + threadIdx.x;
         u64 r[4] = {0, 0, 0, 0};
         u32 mask = 0;
@@ -345,11 +360,15 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
             return false;
         have = p;
     }
-    const u64 blocks_needed = (n + EXP_THREADS - 1) / EXP_THREADS;
-    const int grid = (int)std::min<u64>(blocks_needed, (u64)sm_count());
+    // chunks of up to g_move_window x 1024 boards, no longer than keeps two
+    // chunks per SM
+    const u64 sms = (u64)sm_count();
+    const u32 window = (u32)std::max<u64>(1, std::min<u64>((u64)g_move_window, n / (sms * EXP_THREADS * 2)));
+    const u64 chunks = (n + (u64)window * EXP_THREADS - 1) / ((u64)window * EXP_THREADS);
+    const int grid = (int)std::min<u64>(chunks, sms);
     kclock().begin(s, &kstats().expand_ms);
     expand_moves_kernel<<<grid, EXP_THREADS, EXP_SMEM, s>>>(in, n, out, cap, c.d, t.move, p, d_prune, c.err, ff,
-                                                            plan, c.d + 5);
+                                                            plan, c.d + 5, window);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
     u64 raw = 0;

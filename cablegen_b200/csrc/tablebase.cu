@@ -43,6 +43,7 @@ extern int g_sort_variant;
 extern int g_hash_load_pct;
 extern int g_hash_compact;
 extern int g_region_build;
+extern int g_move_window;
 }
 
 static Engine &E() { return Engine::get(); }
@@ -169,6 +170,12 @@ int cgb_set_option(const char *name, long long value)
             return -1;
         }
         g_region_build = (int)value;
+    } else if (k == "move_window") {
+        if (value < 1 || value > 4) {
+            set_error("cgb_set_option: move_window must be in [1, 4]");
+            return -1;
+        }
+        g_move_window = (int)value;
     } else if (k == "hash_compact") {
         if (value < 0 || value > 1) {
             set_error("cgb_set_option: hash_compact must be 0 or 1");
@@ -209,6 +216,7 @@ long long cgb_get_option(const char *name)
     if (k == "fp64_top_layers") return E().fp64_top_layers;
     if (k == "hash_compact") return g_hash_compact;
     if (k == "region_build") return g_region_build;
+    if (k == "move_window") return g_move_window;
     if (k == "lookback_spin_limit") return g_test_spin;
     if (k == "lookback_hold_first_tile") return g_test_hold;
     if (k == "device_mem_cap_mb") return (long long)(g_dev_mem_cap >> 20);

@@ -54,6 +54,8 @@ int cgb_set_rules(const cgb_rules *rules);
  * "region_build" (1, the default: 16-byte-slot hash indexes of 2^16..2^28 keys
  * built region by region in shared memory; 0: atomic inserts into a zeroed table),
  * "hash_compact" (1, the default: FP32 tables in 8-byte slots where the keys allow),
+ * "move_window" (1..4, default 1: the move expansion drops repeats among the
+ * results of up to this many blocks of 1024 consecutive input boards at once),
  * "fp64_top_layers" (FP32 sweeps of cgb_sweep_run: the highest layers, solved
  * first, whose values come straight from the winstates, are solved in FP64 and
  * narrowed to FP32 for the layers below; default 4, 0 = none).
@@ -66,7 +68,8 @@ long long cgb_get_option(const char *name);
  * src/generate.c:133-175; OpenCL move_kernel, src/cl/generate.cl:249-282).
  * d_out needs cap >= 4n slots; *n_out = boards written (unsorted).  Every
  * distinct result appears at least once; repeats among the results of the same
- * block of 1024 consecutive inputs are written once. */
+ * chunk of consecutive inputs (1024 x "move_window" boards at most) are
+ * written once. */
 int cgb_expand_moves(const uint64_t *d_in, uint64_t n, uint64_t *d_out, uint64_t cap, uint64_t *n_out);
 /* Total number of empty cells (= size of each spawn stream). */
 int cgb_count_spawns(const uint64_t *d_in, uint64_t n, uint64_t *total);

@@ -113,17 +113,18 @@ def test_batch_knobs_do_not_change_results(cuda, batch_case):
     """Every tuned knob value gives the same FP64 tables (the autotuner picks speed only)."""
     w, forms, (want_layers, want_vals) = batch_case
     cuda.set_rules(w.settings)
-    names = ("sort_variant", "solve_variant", "hash_load_pct")
+    names = ("sort_variant", "solve_variant", "hash_load_pct", "move_window")
     old = {k: cuda.get_option(k) for k in names}
     try:
-        for sv, so, hl in ((2, 1, 60), (0, 0, 25), (3, 1, 45), (4, 0, 0)):
+        for sv, so, hl, mw in ((2, 1, 60, 4), (0, 0, 25, 1), (3, 1, 45, 2), (4, 0, 0, 1), (5, 1, 0, 4)):
             cuda.set_option("sort_variant", sv)
             cuda.set_option("solve_variant", so)
             cuda.set_option("hash_load_pct", hl)
+            cuda.set_option("move_window", mw)
             _, tables, _ = cuda.batch(forms, precision=64, keep_tables=True)
             for i in range(len(forms)):
                 for s, vals in want_vals[i].items():
-                    assert np.array_equal(tables[(i, s)][1], vals), (sv, so, hl, i, s)
+                    assert np.array_equal(tables[(i, s)][1], vals), (sv, so, hl, mw, i, s)
     finally:
         for k, v in old.items():
             cuda.set_option(k, v)

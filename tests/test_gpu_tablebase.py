@@ -143,6 +143,29 @@ def test_region_built_index_matches_atomic_build(cuda):
         assert np.array_equal(got[0][s][1], got[1][s][1]), s
 
 
+def test_move_windows_agree(cuda):
+    """Every chunk size of the move expansion's repeat set (1..4 blocks of 1024 boards) gives
+    the same layers: the set only decides how many repeats reach the sort."""
+    w = configs.get("ll_pruned", end_gen=220)
+    f = w.formations[0]
+    cuda.set_rules(w.settings)
+    old = cuda.get_option("move_window")
+    got, kept = {}, {}
+    try:
+        for v in (1, 2, 4):
+            cuda.set_option("move_window", v)
+            before = cuda.kernel_stats()["moves_kept"]
+            got[v], _ = cuda.generate(f.initial, f.start, f.end_gen)
+            kept[v] = cuda.kernel_stats()["moves_kept"] - before
+    finally:
+        cuda.set_option("move_window", old)
+    for v in (2, 4):
+        assert got[v].keys() == got[1].keys()
+        for s in got[1]:
+            assert np.array_equal(got[v][s], got[1][s]), (v, s)
+    assert kept[4] < kept[1]
+
+
 def test_fp32_compact_index_matches_wide(cuda):
     """FP32 tables looked up through 8-byte slots equal those through 16-byte slots, bit for
     bit (both indexes are exact), and the large layers of LL do take the 8-byte form."""

@@ -51,7 +51,7 @@ class FakeDevice:
     """Knob values and a run time that depends on them (the minimum at sort 2, solve 1, load 25)."""
 
     def __init__(self):
-        self.opts = {"sort_variant": 1, "solve_variant": 0, "hash_load_pct": 0}
+        self.opts = {"sort_variant": 1, "solve_variant": 0, "hash_load_pct": 0, "move_window": 1}
         self.runs = 0
 
     def set_option(self, k, v):
@@ -67,7 +67,7 @@ class FakeDevice:
         self.runs += 1
         o = self.opts
         ms = 100 + {3: 8, 4: 9, 5: 11, 1: 10, 0: 5, 2: 0}[o["sort_variant"]] + {0: 7, 1: 0}[o["solve_variant"]] + \
-            {0: 3, 25: 0, 45: 6}[o["hash_load_pct"]]
+            {0: 3, 25: 0, 45: 6}[o["hash_load_pct"]] + {1: 0, 2: 1, 4: 2}[o["move_window"]]
         return {}, {}, {"total_ms": float(ms)}
 
 
@@ -77,13 +77,13 @@ def test_autotune_coordinate_descent_and_cache(monkeypatch, tmp_path):
     monkeypatch.setattr(autotune, "_gpu_name", lambda: "test-gpu")
     cache = str(tmp_path / "tune.json")
     r = autotune.tune("batch64", end_cap=60, precision=32, repeats=1, cache=cache)
-    assert r["params"] == {"sort_variant": 2, "solve_variant": 1, "hash_load_pct": 25}
+    assert r["params"] == {"sort_variant": 2, "solve_variant": 1, "hash_load_pct": 25, "move_window": 1}
     assert r["ms"] == 100.0 and not r["cached"]
     assert fake.opts == r["params"]          # the winners are applied
     assert len(r["trials"]) == 1 + sum(len(v) - 1 for v in autotune.KNOBS.values())
     with open(cache) as f:
         assert "test-gpu|batch64|60|32" in json.load(f)
     runs = fake.runs
-    fake.opts.update(sort_variant=1, solve_variant=0, hash_load_pct=0)
+    fake.opts.update(sort_variant=1, solve_variant=0, hash_load_pct=0, move_window=2)
     again = autotune.tune("batch64", end_cap=60, precision=32, repeats=1, cache=cache)
     assert again["cached"] and fake.runs == runs and fake.opts == r["params"]
