@@ -135,29 +135,15 @@ __device__ __forceinline__ W warp_lookback_sum(const W *words, int j, u32 *err)
         excl += c;
         if (!stop && pre) break;
         j -= __popc(take);
-        if (stop) {
-            if (++spins > limit) {
-                if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
-                break;
-            }
-            __nanosleep(32);
+        // a round trip to L2 per poll is the wait; the poll count bounds it
+        if (stop && ++spins > limit) {
+            if (lane == 0) atomicOr(err, ERR_LOOKBACK_TIMEOUT);
+            break;
         }
     }
     return excl;
 }
 
-// decoupled look-back over one u32 count per tile; returns the exclusive prefix
-__device__ __forceinline__ u32 tile_lookback(u32 *lookback, u32 tile, u32 count, u32 *err)
-{
-    if (tile == 0) {
-        st_relaxed(lookback, LB_PRE | count);
-        return 0;
-    }
-    st_relaxed(lookback + tile, LB_AGG | count);
-    const u32 excl = lookback_sum(lookback, 1, (int)tile - 1, err);
-    st_relaxed(lookback + tile, LB_PRE | (excl + count));
-    return excl;
-}
 
 // ---------------------------------------------------------------------------
 // histogram of all eight byte digits in one pass
@@ -851,15 +837,17 @@ __global__ void __launch_bounds__(UNQ_THREADS, 5) unique_kernel(const u64 *__res
 }
 
 // ---------------------------------------------------------------------------
-// merge path: for output diagonal `diag`, number of elements taken from a
-// (ties go to a first)
-__device__ __forceinline__ u32 merge_path(const u64 *a, u32 na, const u64 *b, u32 nb, u32 diag)
+// merge path over the merge tile's padded shared layout (a[i] at
+// buf[pad8(i)], b[i] at buf[pad8(la + i)]): for output diagonal `diag`, the
+// number of elements taken from a (ties go to a first)
+__device__ __forceinline__ u32 pad8(u32 j) { return j + (j >> 3); }
+__device__ __forceinline__ u32 merge_path_padded(const u64 *buf, u32 la, u32 lb, u32 diag)
 {
-    u32 lo = diag > nb ? diag - nb : 0;
-    u32 hi = diag < na ? diag : na;
+    u32 lo = diag > lb ? diag - lb : 0;
+    u32 hi = diag < la ? diag : la;
     while (lo < hi) {
         const u32 mid = (lo + hi) >> 1;
-        if (a[mid] <= b[diag - 1 - mid]) lo = mid + 1;
+        if (buf[pad8(mid)] <= buf[pad8(la + diag - 1 - mid)]) lo = mid + 1;
         else hi = mid;
     }
     return lo;
@@ -870,34 +858,6 @@ __device__ __forceinline__ u32 merge_path(const u64 *a, u32 na, const u64 *b, u3
 constexpr u64 LB64_AGG = 1ull << 62, LB64_PRE = 2ull << 62, LB64_MASK = (1ull << 62) - 1;
 
 
-__device__ __forceinline__ u64 tile_lookback64(u64 *lookback, u32 tile, u64 count, u32 *err)
-{
-    if (tile == 0) {
-        st_relaxed64(lookback, LB64_PRE | count);
-        return 0;
-    }
-    st_relaxed64(lookback + tile, LB64_AGG | count);
-    u64 excl = 0;
-    int j = (int)tile - 1;
-    u32 spins = 0;
-    while (j >= 0) {
-        const u64 v = ld_relaxed64(lookback + j);
-        const u64 flag = v & ~LB64_MASK;
-        if (flag == 0) {
-            if (++spins > g_spin_limit) {
-                atomicOr(err, ERR_LOOKBACK_TIMEOUT);
-                break;
-            }
-            __nanosleep(32);
-            continue;
-        }
-        excl += v & LB64_MASK;
-        if (flag == LB64_PRE) break;
-        j--;
-    }
-    st_relaxed64(lookback + tile, LB64_PRE | (excl + count));
-    return excl;
-}
 
 __device__ __forceinline__ u64 merge_path64(const u64 *a, u64 na, const u64 *b, u64 nb, u64 diag)
 {
@@ -958,7 +918,7 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
 #pragma unroll
         for (int i = 0; i < MRG_KPT; i++) {
             const u32 j = i * MRG_THREADS + threadIdx.x;
-            if (j < la + lb) buf[j] = r[i];
+            if (j < la + lb) buf[pad8(j)] = r[i];
         }
     }
     // the merged element just before this tile
@@ -970,13 +930,14 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
         else before = max(a[a0 - 1], b[b0 - 1]);
     }
     __syncthreads();
-    const u64 *sa = buf, *sb = buf + la;
+    // a thread's runs start about MRG_KPT / 2 keys apart in each input: the
+    // padded layout spreads their reads over the banks
     const u32 len = (u32)(d1 - d0);
     const u32 t0 = min((u32)(threadIdx.x * MRG_KPT), len);
     const u32 t1 = min(t0 + MRG_KPT, len);
-    u32 ia = merge_path(sa, la, sb, lb, t0);
+    u32 ia = merge_path_padded(buf, la, lb, t0);
     u32 ib = t0 - ia;
-    u64 xa = ia < la ? sa[ia] : 0ull, xb = ib < lb ? sb[ib] : 0ull;
+    u64 xa = ia < la ? buf[pad8(ia)] : 0ull, xb = ib < lb ? buf[pad8(la + ib)] : 0ull;
     u64 v[MRG_KPT];
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++) {
@@ -985,11 +946,11 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
             if (take_a) {
                 v[i] = xa;
                 ++ia;
-                xa = ia < la ? sa[ia] : 0ull;
+                xa = ia < la ? buf[pad8(ia)] : 0ull;
             } else {
                 v[i] = xb;
                 ++ib;
-                xb = ib < lb ? sb[ib] : 0ull;
+                xb = ib < lb ? buf[pad8(la + ib)] : 0ull;
             }
         } else {
             v[i] = 0ull;
@@ -1051,14 +1012,14 @@ __global__ void __launch_bounds__(MRG_THREADS) merge_unique_kernel(const u64 *__
 #pragma unroll
     for (int i = 0; i < MRG_KPT; i++)
         if (flags & (1u << i)) {
-            buf[w + (w >> 3)] = v[i];
+            buf[pad8(w)] = v[i];
             w++;
         }
     __syncthreads();
     const u64 prefix = prefix_sh;
     const u32 kept = kept_sh;
     for (u32 j = threadIdx.x; j < kept; j += MRG_THREADS) {
-        if (prefix + j < total) out[prefix + j] = buf[j + (j >> 3)];
+        if (prefix + j < total) out[prefix + j] = buf[pad8(j)];
         else atomicOr(err, ERR_CAPACITY);
     }
 }
