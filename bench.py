@@ -393,7 +393,11 @@ def run_ours(args):
     gen_k = sum(kst[f"{f}_ms"] for f in ("expand", "spawn", "onesweep", "hist", "unique", "merge"))
     sol_k = kst["solve_ms"] + kst["index_ms"]
     phases = {"gen_ms": sum(s["gen_ms"] for s in stats) / k, "gen_kernel_ms": gen_k / k,
-              "solve_ms": sum(s["solve_ms"] for s in stats) / k, "solve_kernel_ms": sol_k / k}
+              "solve_ms": sum(s["solve_ms"] for s in stats) / k, "solve_kernel_ms": sol_k / k,
+              "step_ms": [round(s["total_ms"], 1) for s in stats],
+              # resident-layer chunks moved to pinned host memory and back (the store's spill policy)
+              "spilled_chunks": sum(s.get("spilled_chunks", 0) for s in stats),
+              "restored_chunks": sum(s.get("restored_chunks", 0) for s in stats)}
 
     # ---- FP32 sweep, its error against FP64, and the plain (bisection) FP64 solve
     fp32 = None
