@@ -397,7 +397,8 @@ def run_ours(args):
               "step_ms": [round(s["total_ms"], 1) for s in stats],
               # resident-layer chunks moved to pinned host memory and back (the store's spill policy)
               "spilled_chunks": sum(s.get("spilled_chunks", 0) for s in stats),
-              "restored_chunks": sum(s.get("restored_chunks", 0) for s in stats)}
+              "restored_chunks": sum(s.get("restored_chunks", 0) for s in stats),
+              "pool_trims": kst.get("pool_trims", 0)}
 
     # ---- FP32 sweep, its error against FP64, and the plain (bisection) FP64 solve
     fp32 = None

@@ -51,7 +51,7 @@ class KernelStats(C.Structure):
                                              "solve")] + \
         [("onesweep_launches", C.c_uint64), ("solve_launches", C.c_uint64), ("solve_boards", C.c_uint64),
          ("lookups", C.c_uint64), ("index_builds", C.c_uint64), ("compact_index_builds", C.c_uint64),
-         ("moves_raw", C.c_uint64), ("moves_kept", C.c_uint64)]
+         ("moves_raw", C.c_uint64), ("moves_kept", C.c_uint64), ("pool_trims", C.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

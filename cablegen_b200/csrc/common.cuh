@@ -47,6 +47,7 @@ struct KernelStats {
     u64 onesweep_launches = 0, solve_launches = 0, solve_boards = 0, lookups = 0;
     u64 index_builds = 0, compact_index_builds = 0;
     u64 moves_raw = 0, moves_kept = 0;  // move results before / after the per-block set
+    u64 pool_trims = 0;  // failed allocations that returned the pool's cache to the device
 };
 KernelStats &kstats();
 

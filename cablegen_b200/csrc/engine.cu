@@ -136,6 +136,7 @@ bool dev_alloc(void **p, u64 bytes, cudaStream_t s)
         cudaGetDevice(&dev);
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        kstats().pool_trims++;
         e = cudaMallocAsync(p, bytes, s);
     }
     if (e != cudaSuccess) {

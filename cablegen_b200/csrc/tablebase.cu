@@ -84,6 +84,7 @@ int cgb_get_kernel_stats(cgb_kernel_stats *o)
     o->compact_index_builds = k.compact_index_builds;
     o->moves_raw = k.moves_raw;
     o->moves_kept = k.moves_kept;
+    o->pool_trims = k.pool_trims;
     return 0;
 }
 

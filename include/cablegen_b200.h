@@ -141,7 +141,10 @@ typedef struct {
     uint64_t hist_bytes, onesweep_bytes, unique_bytes, merge_bytes, expand_bytes, spawn_bytes, solve_bytes;
     uint64_t onesweep_launches, solve_launches, solve_boards, lookups;
     uint64_t index_builds, compact_index_builds;  /* hash indexes built; of them in 8-byte slots */
-    uint64_t moves_raw, moves_kept;  /* move results before / after dropping repeats per 1024-board block */
+    uint64_t moves_raw, moves_kept;  /* move results before / after dropping repeats per chunk of
+                                        1024 x "move_window" consecutive boards */
+    uint64_t pool_trims;  /* device allocations that failed, returned the allocator's cached
+                             blocks to the device and were retried */
 } cgb_kernel_stats;
 int cgb_get_kernel_stats(cgb_kernel_stats *out);
 int cgb_reset_kernel_stats(void);
