@@ -47,7 +47,7 @@ FALLBACK_HBM_GBS = 6650.0
 # (smaller cases of the same kernels; their traffic grows in proportion to the units):
 # a sort digit pass per key (onesweep_byte512_88M_ll_keys.md), the solve per board
 # (solve_items_f64_ll_layer196.md).
-NCU_DRAM_BYTES_PER_UNIT = {"onesweep": 1.384571e9 / 88333334, "solve": 1.915215e9 / 5404078}
+NCU_DRAM_BYTES_PER_UNIT = {"onesweep": 1.379122e9 / 88333334, "solve": 1.915215e9 / 5404078}
 
 
 def parse():
