@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that holds the reference sources; their path comes from the
-CABLEGEN_REFERENCE environment variable, else BASELINE.json's "reference_path":
+Run in a container that holds the reference sources, built into oracle/_ref first
+(their path: REF=<dir> or the CABLEGEN_REFERENCE environment variable):
 
     make -C oracle all REF=<reference sources> # builds oracle/_ref/{libcgref.so,cli}
     python tests/golden/make_golden.py units
