@@ -400,6 +400,30 @@ def run_ours(args):
               "restored_chunks": sum(s.get("restored_chunks", 0) for s in stats),
               "pool_trims": kst.get("pool_trims", 0)}
 
+    # ---- like for like with the reference arm: the same sample (generate + solve over
+    # the reference arm's tile sums) through the drop-in C API, every file written.  It runs
+    # right after the timed sweep, as in a CLI user's fresh process: placed after the FP32
+    # block it measured 1.0e8 boards/s on a B200, right after the timed sweep 1.95e8 (same
+    # code), its file writes slowed by the host memory the earlier blocks had touched
+    like = None
+    if not args.no_e2e and rank == 0:
+        cend = args.cpu_end or default_cpu_end(args.workload)
+        dropin_sample(args.workload, cend)  # warm-up
+        db, dsec, dbytes = 0, 0.0, 0
+        for _ in range(max(1, min(args.steps, 5))):
+            b, dt, nb = dropin_sample(args.workload, cend)
+            db += b
+            dsec += dt
+            dbytes = nb
+        device.set_rules(wl.settings)
+        like = {"value": db / dsec, "unit": "boards/s", "end_gen": cend,
+                "sample": f"generate {form.start}..{cend} then solve {cend}..{form.start} of {args.workload}, "
+                          "the reference arm's sample",
+                "path": "include/cablegen.h generate() + solve() (the calls the reference CLI makes), "
+                        ".boards and .tables files written to /dev/shm",
+                "bytes_written_per_step": dbytes, "h2d_bytes_per_step": 8 * len(form.initial),
+                "d2h_bytes_per_step": dbytes}
+
     # ---- FP32 sweep, its error against FP64, and the plain (bisection) FP64 solve
     fp32 = None
     if not args.no_fp32:
@@ -429,28 +453,6 @@ def run_ours(args):
             fp32["solve_speedup_vs_plain_fp64"] = fp32["solve_boards_per_s"] / fp32["plain_fp64_solve_boards_per_s"]
         if fp32["solve_boards_per_s"] and fp32["fp64_solve_boards_per_s"]:
             fp32["solve_speedup_vs_fp64_hash"] = fp32["solve_boards_per_s"] / fp32["fp64_solve_boards_per_s"]
-
-    # ---- like for like with the reference arm: the same sample (generate + solve over
-    # the reference arm's tile sums) through the drop-in C API, every file written (before
-    # the e2e block, which keeps tens of GB of host memory pinned for its layer copies)
-    like = None
-    if not args.no_e2e and rank == 0:
-        cend = args.cpu_end or default_cpu_end(args.workload)
-        dropin_sample(args.workload, cend)  # warm-up
-        db, dsec, dbytes = 0, 0.0, 0
-        for _ in range(max(1, min(args.steps, 5))):
-            b, dt, nb = dropin_sample(args.workload, cend)
-            db += b
-            dsec += dt
-            dbytes = nb
-        device.set_rules(wl.settings)
-        like = {"value": db / dsec, "unit": "boards/s", "end_gen": cend,
-                "sample": f"generate {form.start}..{cend} then solve {cend}..{form.start} of {args.workload}, "
-                          "the reference arm's sample",
-                "path": "include/cablegen.h generate() + solve() (the calls the reference CLI makes), "
-                        ".boards and .tables files written to /dev/shm",
-                "bytes_written_per_step": dbytes, "h2d_bytes_per_step": 8 * len(form.initial),
-                "d2h_bytes_per_step": dbytes}
 
     # ---- end to end through the C ABI: every layer and every table copied to host buffers
     e2e = None
