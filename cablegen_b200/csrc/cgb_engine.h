@@ -116,6 +116,10 @@ struct GenBuffers {
     DevBuf<u64> u2, u4, u4_next;
     DevBuf<u64> moved;         // the current layer
     DevBuf<u64> t;             // merge scratch of sliced layer steps
+    // empty cells over the moved layer (the size of its spawn streams), counted by
+    // the move step's unique pass; unknown after a sliced move step
+    u64 moved_empties = 0;
+    bool moved_empties_known = false;
 };
 
 struct Engine {
@@ -125,6 +129,10 @@ struct Engine {
     DeviceRowTable rt;
     SortWorkspace ws;
     Counters ctr;
+    // pinned words the spawn expansion's count and error word are copied into
+    // without a wait, and the event after that copy (checked at a later wait)
+    u64 *h_spawn_check = nullptr;
+    cudaEvent_t spawn_check_ev = nullptr;
     cgb_rules rules{};
     int index_kind = INDEX_HASH;  // lookup structure of solved layers
     int bucket_bits = 22;         // INDEX_BUCKET: bucket count = 2^bits
@@ -148,7 +156,8 @@ struct Engine {
     bool move_layer(const u64 *d_in, u64 n, GenTimes *tm);
     bool spawn_layer(GenTimes *tm, bool unique_streams = false);
     bool sort_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, DevBuf<u64> **out, GenTimes *tm);
-    bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm);
+    bool sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm,
+                          u64 *empties = nullptr);
     bool merge_into(DevBuf<u64> &acc, const u64 *run, u64 n);
     // layers start..end from the input set of layer `start`; h_carry = the
     // 4-spawns of layer start-2 still to merge into layer start+2's input

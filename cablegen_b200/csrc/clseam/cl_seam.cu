@@ -85,6 +85,7 @@ bool move_to(const uint64_t *boards, size_t n, bool prune, long stsl, long ltc, 
     drop(in, E().stream);
     if (!ok) return false;
     std::swap(*out, E().gen.moved);
+    E().gen.moved_empties_known = false;  // the count left with the layer
     note_vram();
     return E().sync();
 }
@@ -94,6 +95,7 @@ bool spawn_from(DevBuf<u64> &in, DevBuf<u64> *n2, DevBuf<u64> *n4)
 {
     if (!E().ready) return false;
     std::swap(E().gen.moved, in);
+    E().gen.moved_empties_known = false;  // a layer from outside: its spawns are counted
     drop(in, E().stream);  // the engine's previous layer buffer
     if (!E().spawn_layer(nullptr, true)) return false;  // the seam's contract: unique streams
     std::swap(*n2, E().gen.u2);

@@ -314,6 +314,13 @@ bool Engine::init(int dev)
     // that fails returns the cache to the device and retries (dev_alloc)
     u64 keep = ~0ull;
     if (!CGB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep))) return false;
+    if (!h_spawn_check) {
+        void *h = nullptr;
+        if (!CGB_CUDA(cudaHostAlloc(&h, 2 * sizeof(u64), cudaHostAllocDefault))) return false;
+        h_spawn_check = (u64 *)h;
+        h_spawn_check[0] = h_spawn_check[1] = 0;
+    }
+    if (!spawn_check_ev && !CGB_CUDA(cudaEventCreateWithFlags(&spawn_check_ev, cudaEventDisableTiming))) return false;
     if (!ctr.d) {
         void *p;
         if (!CGB_CUDA(cudaMalloc(&p, 64 * sizeof(u64)))) return false;
@@ -353,7 +360,8 @@ static bool reserve(DevBuf<u64> &b, u64 n, cudaStream_t s)
 
 // sort + unique of n raw keys in x (y = scratch); returns the buffer holding
 // the unique keys (the other one is left free)
-bool Engine::sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm)
+bool Engine::sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, DevBuf<u64> **out, GenTimes *tm,
+                              u64 *empties)
 {
     cudaStream_t s = stream;
     u64 *sorted = x.p;
@@ -365,7 +373,7 @@ bool Engine::sort_unique_step(DevBuf<u64> &x, DevBuf<u64> &y, u64 n, u64 *nu, De
     }
     DevBuf<u64> &full = (sorted == x.p) ? x : y;
     DevBuf<u64> &dst = (sorted == x.p) ? y : x;
-    if (!unique_keys(full.p, n, dst.p, nu, ws, s)) return false;
+    if (!unique_keys(full.p, n, dst.p, nu, ws, s, empties)) return false;
     *out = &dst;
     return true;
 }
@@ -409,16 +417,19 @@ bool Engine::move_layer(const u64 *d_in, u64 n, GenTimes *tm)
     const u64 m0 = chunked ? slice : n;
     if (!reserve(g.a, 4 * m0, s) || !reserve(g.b, 4 * m0, s)) return false;
     if (chunked) g.moved.n = 0;
+    g.moved_empties_known = false;
     for (u64 off = 0; off < n || (n == 0 && off == 0); off += m0) {
         const u64 m = std::min(m0, n - off);
         u64 nr = 0;
         if (!expand_moves(d_in + off, m, g.a.p, 4 * m, &nr, rt, prune_params(), ctr, s, filter, plan)) return false;
-        u64 nu = 0;
+        u64 nu = 0, empties = 0;
         DevBuf<u64> *u = nullptr;
-        if (!sort_unique_step(g.a, g.b, nr, &nu, &u, tm)) return false;
+        if (!sort_unique_step(g.a, g.b, nr, &nu, &u, tm, chunked ? nullptr : &empties)) return false;
         if (!chunked) {
             std::swap(*u, g.moved);   // the layer; the old layer buffer becomes scratch
             g.moved.n = nu;
+            g.moved_empties = empties;
+            g.moved_empties_known = true;
             return true;
         }
         if (!merge_into(g.moved, u->p, nu)) return false;
@@ -437,8 +448,11 @@ bool Engine::spawn_layer(GenTimes *tm, bool unique_streams)
     GenBuffers &g = gen;
     const u64 *d_moved = g.moved.p;
     const u64 n = g.moved.n;
+    // the spawn total: counted by the move step's unique pass, else by a kernel
     u64 total = 0;
-    if (!count_spawns(d_moved, n, &total, ctr, s)) return false;
+    if (g.moved_empties_known) total = g.moved_empties;
+    else if (!count_spawns(d_moved, n, &total, ctr, s)) return false;
+    g.moved_empties_known = false;  // it belongs to this layer only
     const bool chunked = total > max_sort_keys;
     const u64 cap = chunked ? max_sort_keys : total;
     for (auto &x : g.c)
@@ -461,7 +475,18 @@ bool Engine::spawn_layer(GenTimes *tm, bool unique_streams)
             }
         }
         u64 ns = 0;
-        if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s, plan)) return false;
+        // one slice: the streams hold exactly t keys each; the kernel's count and
+        // error word are checked after the first sort below has waited on the
+        // stream anyway.  Slices keep the synchronous check.
+        const bool deferred = !chunked;
+        if (deferred) {
+            if (!expand_spawns_deferred(d_moved + off, m, g.c[0].p, g.c[1].p, t, ctr, s, plan, h_spawn_check,
+                                        spawn_check_ev))
+                return false;
+            ns = t;
+        } else if (!expand_spawns(d_moved + off, m, g.c[0].p, g.c[1].p, t, &ns, ctr, s, plan)) {
+            return false;
+        }
         // the 2-spawns sort c[0] with c[2] as scratch; the 4-spawns then sort
         // c[1] with the buffer the first sort left free.  Without unique_streams
         // the sorted streams keep their repeats: every later merge drops them
@@ -472,6 +497,7 @@ bool Engine::spawn_layer(GenTimes *tm, bool unique_streams)
         } else if (!sort_step(g.c[0], g.c[2], ns, &u2, tm)) {
             return false;
         }
+        if (deferred && !check_spawns_deferred(h_spawn_check, spawn_check_ev, t)) return false;
         DevBuf<u64> &spare = (u2 == &g.c[0]) ? g.c[2] : g.c[0];
         if (unique_streams) {
             if (!sort_unique_step(g.c[1], spare, ns, &n4, &u4, tm)) return false;

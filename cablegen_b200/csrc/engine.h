@@ -33,7 +33,9 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
 // reports device errors a sort left behind (when no unique_keys follows)
 bool sort_check(SortWorkspace &ws, cudaStream_t s);
 // out must not alias in
-bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s);
+// empties (optional): the number of empty cells over the kept keys
+bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s,
+                 u64 *empties = nullptr);
 // sorted union of two sorted runs, without repeats (repeats inside a run are
 // dropped as well)
 bool merge_unique(const u64 *a, u64 na, const u64 *b, u64 nb, u64 *out, u64 *n_out, SortWorkspace &ws,
@@ -64,6 +66,11 @@ bool expand_moves(const u64 *in, u64 n, u64 *out, u64 cap, u64 *n_out, const Dev
                   const CanonPlan &plan = CanonPlan{});
 // number of empty cells over all boards (exact size of the spawn streams)
 bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s);
+// expand_spawns with cap = the exact spawn total and no wait: its count and error
+// word land in h_check (pinned, 2 words) behind `done`, for check_spawns_deferred
+bool expand_spawns_deferred(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, Counters &c, cudaStream_t s,
+                            const CanonPlan &plan, u64 *h_check, cudaEvent_t done);
+bool check_spawns_deferred(const u64 *h_check, cudaEvent_t done, u64 expect);
 // canonical 2-spawn and 4-spawn of every empty cell of every board
 bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c,
                    cudaStream_t s, const CanonPlan &plan = CanonPlan{});

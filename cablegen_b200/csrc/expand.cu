@@ -396,6 +396,45 @@ bool count_spawns(const u64 *in, u64 n, u64 *total, Counters &c, cudaStream_t s)
     return true;
 }
 
+// expand_spawns without the wait: the count and the error word are copied into
+// h_check (pinned, two words) behind the kernel and `done` is recorded after the
+// copy; check_spawns_deferred reads them once the caller has waited anyway
+bool expand_spawns_deferred(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, Counters &c, cudaStream_t s,
+                            const CanonPlan &plan, u64 *h_check, cudaEvent_t done)
+{
+    if (!CGB_CUDA(cudaMemsetAsync(c.d, 0, sizeof(u64), s))) return false;
+    if (!CGB_CUDA(cudaMemsetAsync(c.err, 0, sizeof(u32), s))) return false;
+    if (n) {
+        const int grid = (int)std::min<u64>((n + 255) / 256, (u64)sm_count() * 8);
+        kclock().begin(s, &kstats().spawn_ms);
+        expand_spawns_kernel<<<grid, 256, 0, s>>>(in, n, out2, out4, cap, c.d, c.err, plan);
+        kclock().end(s);
+        if (!CGB_CUDA(cudaGetLastError())) return false;
+    }
+    if (!CGB_CUDA(cudaMemcpyAsync(h_check, c.d, sizeof(u64), cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaMemcpyAsync(h_check + 1, c.err, sizeof(u32), cudaMemcpyDeviceToHost, s)) ||
+        !CGB_CUDA(cudaEventRecord(done, s)))
+        return false;
+    kstats().spawn_bytes += 8 * n + 16 * cap;
+    return true;
+}
+
+bool check_spawns_deferred(const u64 *h_check, cudaEvent_t done, u64 expect)
+{
+    if (!CGB_CUDA(cudaEventSynchronize(done))) return false;
+    const u32 e = (u32)h_check[1];
+    if (e) {
+        set_error(std::string("expand_spawns: device error ") + err_string(e));
+        return false;
+    }
+    if (h_check[0] != expect) {
+        set_error("expand_spawns: " + std::to_string(h_check[0]) + " spawns written, " + std::to_string(expect) +
+                  " expected");
+        return false;
+    }
+    return true;
+}
+
 bool expand_spawns(const u64 *in, u64 n, u64 *out2, u64 *out4, u64 cap, u64 *n_out, Counters &c, cudaStream_t s,
                    const CanonPlan &plan)
 {

@@ -39,7 +39,7 @@ __global__ void digit_histogram_kernel(const u64 *__restrict__ keys, u64 n, u32 
 __global__ void onesweep_kernel(const u64 *__restrict__ src, u64 *__restrict__ dst, u32 n, int shift,
                                 const u32 *__restrict__ digit_hist, u32 *lookback, u32 *tile_counter, u32 *err);
 __global__ void unique_kernel(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out, u32 *lookback,
-                              u32 *tile_counter, u32 *out_count, u32 *err);
+                              u32 *tile_counter, u32 *out_count, u32 *err, unsigned long long *empties);
 int sort_plan(const u32 *hist_host, u64 n, int *digits);
 
 namespace noalloc {
@@ -132,7 +132,7 @@ extern "C" int cgb_sort_unique_noalloc(const uint64_t *d_in, uint64_t n, uint64_
         src = dst;
     }
     if (!CGB_CUDA(cudaMemsetAsync(lookback, 0, (u64)tiles * sizeof(u32), s))) return -1;
-    unique_kernel<<<tiles, 256, 0, s>>>(src, (u32)n, d_out, lookback, ctr + 8, count, err);
+    unique_kernel<<<tiles, 256, 0, s>>>(src, (u32)n, d_out, lookback, ctr + 8, count, err, nullptr);
     if (!CGB_CUDA(cudaGetLastError())) return -1;
     u32 res[2];
     if (!CGB_CUDA(cudaMemcpyAsync(res, err, 2 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return -1;

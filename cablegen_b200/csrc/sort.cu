@@ -761,9 +761,17 @@ struct UniqueSmem {
     u32 tile;
 };
 
+// empty cells (0 nibbles) of a board
+__device__ __forceinline__ u32 zero_nibbles(u64 k)
+{
+    const u64 x = k | (k >> 1) | (k >> 2) | (k >> 3);
+    return (u32)__popcll(~x & 0x1111111111111111ull);
+}
+
 template <bool FULL>
 __device__ __forceinline__ void unique_tile(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out, u32 *lookback,
-                                            u32 tile, u32 *out_count, u32 *err, UniqueSmem &S)
+                                            u32 tile, u32 *out_count, u32 *err, UniqueSmem &S,
+                                            unsigned long long *empties)
 {
     constexpr u32 ALL = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -813,27 +821,36 @@ __device__ __forceinline__ void unique_tile(const u64 *__restrict__ in, u32 n, u
     __syncthreads();
     u32 pos = S.warp_base[warp];
     const u32 lt = lanemask_lt();
+    u32 ecount = 0;  // empty cells of this thread's kept keys (when asked for)
 #pragma unroll
     for (int q = 0; q < UNQ_KPT; q++) {
         if ((mask[q] >> lane) & 1) {
             const u32 g = pos + __popc(mask[q] & lt);
-            if (g < n) out[g] = S.keys[1 + wfirst + q * 32 + lane];
+            const u64 v = S.keys[1 + wfirst + q * 32 + lane];
+            if (empties) ecount += zero_nibbles(v);
+            if (g < n) out[g] = v;
             else atomicOr(err, ERR_CAPACITY);
         }
         pos += __popc(mask[q]);
     }
+    if (empties) {
+        const u32 w = __reduce_add_sync(0xffffffffu, ecount);
+        if (lane == 0 && w) atomicAdd(empties, (unsigned long long)w);
+    }
 }
 
+// empties: null, or a word that receives the number of empty cells over the
+// kept keys (boards) -- the size of their spawn streams
 __global__ void __launch_bounds__(UNQ_THREADS, 5) unique_kernel(const u64 *__restrict__ in, u32 n, u64 *__restrict__ out,
                                                                 u32 *lookback, u32 *tile_counter, u32 *out_count,
-                                                                u32 *err)
+                                                                u32 *err, unsigned long long *empties)
 {
     __shared__ UniqueSmem S;
     if (threadIdx.x == 0) S.tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const u32 tile = S.tile;
-    if ((u64)(tile + 1) * UNQ_TILE <= n) unique_tile<true>(in, n, out, lookback, tile, out_count, err, S);
-    else unique_tile<false>(in, n, out, lookback, tile, out_count, err, S);
+    if ((u64)(tile + 1) * UNQ_TILE <= n) unique_tile<true>(in, n, out, lookback, tile, out_count, err, S, empties);
+    else unique_tile<false>(in, n, out, lookback, tile, out_count, err, S, empties);
 }
 
 // ---------------------------------------------------------------------------
@@ -1056,7 +1073,8 @@ void SortWorkspace::release(cudaStream_t s)
 
 // small words: [0,2048) histograms, [2048,2064) tile counters, 2064 err, 2065 count,
 // 2066-2067 a 64-bit count (8-byte aligned)
-static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065, W_COUNT64 = 2066, W_OFFS = 4096;
+static constexpr int W_HIST = 0, W_CTR = 2048, W_ERR = 2064, W_COUNT = 2065, W_COUNT64 = 2066, W_EMPTIES = 2068,
+                     W_OFFS = 4096;
 
 static bool check_err(SortWorkspace &ws, cudaStream_t s, const char *what)
 {
@@ -1179,9 +1197,10 @@ bool sort_keys(u64 *keys, u64 *tmp, u64 n, u64 **sorted, SortWorkspace &ws, cuda
     return true;
 }
 
-bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s)
+bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, cudaStream_t s, u64 *empties)
 {
     *n_out = 0;
+    if (empties) *empties = 0;
     if (n == 0) return true;
     if (n > (u64)LB_MASK) {
         set_error("unique_keys: more than 2^30 keys in one call");
@@ -1190,17 +1209,19 @@ bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, 
     if (!ws.reserve((n + UNQ_TILE - 1) / UNQ_TILE + 1, s)) return false;
     const u32 tiles = ceil_div(n, UNQ_TILE);
     if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_CTR, 0, (W_ERR - W_CTR) * sizeof(u32), s))) return false;
-    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_COUNT, 0, sizeof(u32), s))) return false;
+    // the count, the 64-bit count slot and the empty-cell sum start at zero
+    if (!CGB_CUDA(cudaMemsetAsync(ws.small + W_COUNT, 0, (W_EMPTIES + 2 - W_COUNT) * sizeof(u32), s))) return false;
     if (!ws.err_dirty && !CGB_CUDA(cudaMemsetAsync(ws.small + W_ERR, 0, sizeof(u32), s))) return false;
     ws.err_dirty = false;
     if (!CGB_CUDA(cudaMemsetAsync(ws.lookback, 0, (u64)tiles * sizeof(u32), s))) return false;
     kclock().begin(s, &kstats().unique_ms);
     unique_kernel<<<tiles, UNQ_THREADS, 0, s>>>(in, (u32)n, out, ws.lookback, ws.small + W_CTR,
-                                                ws.small + W_COUNT, ws.small + W_ERR);
+                                                ws.small + W_COUNT, ws.small + W_ERR,
+                                                empties ? (unsigned long long *)(ws.small + W_EMPTIES) : nullptr);
     kclock().end(s);
     if (!CGB_CUDA(cudaGetLastError())) return false;
-    u32 ec[2];  // error word, count
-    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, 2 * sizeof(u32), cudaMemcpyDeviceToHost, s))) return false;
+    u32 ec[W_EMPTIES + 2 - W_ERR];  // error word, count, (64-bit count), empty-cell sum
+    if (!CGB_CUDA(cudaMemcpyAsync(ec, ws.small + W_ERR, sizeof(ec), cudaMemcpyDeviceToHost, s))) return false;
     if (!CGB_CUDA(cudaStreamSynchronize(s))) return false;
     kclock().flush();
     if (ec[0]) {
@@ -1210,6 +1231,7 @@ bool unique_keys(const u64 *in, u64 n, u64 *out, u64 *n_out, SortWorkspace &ws, 
     const u32 cnt = ec[1];
     kstats().unique_bytes += 8 * (n + cnt);
     *n_out = cnt;
+    if (empties) memcpy(empties, &ec[W_EMPTIES - W_ERR], sizeof(u64));
     return true;
 }
 
