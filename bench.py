@@ -122,6 +122,13 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def wait_first(self, timeout=10.0):
+        """Block until the first sample arrived, so that nvidia-smi's start-up (a burst of
+        host work) lies before the timed region, not inside it."""
+        t_end = time.time() + timeout
+        while self.proc and not self.samples and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.02)
+
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
@@ -373,10 +380,11 @@ def run_ours(args):
     for _ in range(args.warmup):
         step(64)
 
-    # ---- timed region: K steps of the FP64 sweep
-    barrier()
+    # ---- timed region: K steps of the FP64 sweep (the clock sampler is running before it starts)
     clocks = ClockSampler(dev)
     clocks.start()
+    clocks.wait_first()
+    barrier()
     device.reset_kernel_stats()
     t0 = time.perf_counter()
     stats = [step(64) for _ in range(args.steps)]
