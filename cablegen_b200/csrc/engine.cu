@@ -6,9 +6,11 @@
 //          carried to become part of n2)
 // and per layer runs
 //   moved = unique(sort(expand_moves(S_s)))           -> the layer s.boards
-//   U2    = unique(sort(spawn2(moved)))
-//   U4'   = unique(sort(spawn4(moved)))
+//   U2    = sort(spawn2(moved))                        (repeats kept)
+//   U4'   = sort(spawn4(moved))                        (repeats kept)
 //   S_s+2 = merge_unique(U2, U4)                       (src/generate.c:530-544)
+// (the merge drops repeats inside its runs as well as across them; the unique
+// pass of the move step also counts the spawns the next step will make)
 // Layers go to a LayerSink: it keeps them in HBM (the resident gen+solve
 // run) or copies them out (files through the C API).
 //
