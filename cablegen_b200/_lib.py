@@ -125,6 +125,7 @@ def _declare(L):
         "cgb_get_kernel_stats": (C.c_int, [C.POINTER(KernelStats)]),
         "cgb_reset_kernel_stats": (C.c_int, []),
         "cgb_solve_layer": (C.c_int, [vp, u64, vp, C.c_int, vp, vp, u64, vp, vp, u64, pu64, C.c_int]),
+        "cgb_lookup_batch": (C.c_int, [vp, vp, u64, C.c_int, vp, u64, C.c_int, vp]),
         "cgb_generate": (C.c_int, [pu64, u64, C.c_int, C.c_int, LAYER_FN, vp, C.POINTER(Stats)]),
         "cgb_sweep_run": (C.c_int, [C.POINTER(Sweep), C.POINTER(Stats)]),
         "cgb_batch_run": (C.c_int, [C.POINTER(Batch), C.POINTER(BatchStats)]),

@@ -129,6 +129,10 @@ bool build_hash_enqueue(LayerIndex &ix, int vbytes, void *slots, u64 cap, u32 *e
 // builds ix (keys/vals/n already set) of the requested kind; vbytes = 8 or 4
 bool build_index(LayerIndex &ix, int kind, int vbytes, IndexStorage &st, int bucket_bits, Counters &c,
                  cudaStream_t s);
+// the value of each of m boards (canonicalised first when canon) in an indexed
+// layer, widened to double; 0.0 for a board not in it
+bool lookup_batch(const LayerIndex &ix, int vbytes, const u64 *boards, u64 m, bool canon, double *out,
+                  cudaStream_t s);
 
 // plan: images that can be canonical for the layer's 0xf mask (CanonPlan{}: all eight)
 bool solve_layer_f64(const u64 *keys, u64 n, double *out, const LayerIndex &t2, const LayerIndex &t4,

@@ -960,4 +960,28 @@ bool solve_layer_f32(const u64 *keys, u64 n, float *out, const LayerIndex &t2, c
     return launch_solve<float>(keys, n, out, t2, t4, r, rt, c, s, plan);
 }
 
+// ---- batch lookup (lookup(), src/solve.c:108-164, for many boards) --------
+template <typename V>
+__global__ void __launch_bounds__(256) lookup_batch_kernel(DevTable<V> t, const u64 *__restrict__ boards, u64 m,
+                                                           int canon, double *__restrict__ out)
+{
+    for (u64 i = (u64)blockIdx.x * 256 + threadIdx.x; i < m; i += (u64)gridDim.x * 256) {
+        const u64 b = boards[i];
+        out[i] = (double)table_value(t, canon ? canonical(b) : b);
+    }
+}
+
+bool lookup_batch(const LayerIndex &ix, int vbytes, const u64 *boards, u64 m, bool canon, double *out,
+                  cudaStream_t s)
+{
+    if (m == 0) return true;
+    const int grid = grid_for(m, 256, 8);
+    if (vbytes == 4)
+        lookup_batch_kernel<float><<<grid, 256, 0, s>>>(dev_table<float>(ix), boards, m, canon ? 1 : 0, out);
+    else
+        lookup_batch_kernel<double><<<grid, 256, 0, s>>>(dev_table<double>(ix), boards, m, canon ? 1 : 0, out);
+    kstats().launches++;
+    return CGB_CUDA(cudaGetLastError());
+}
+
 }  // namespace cgb

@@ -371,6 +371,29 @@ extern "C" int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, 
     return 0;
 }
 
+int cgb_lookup_batch(const uint64_t *d_keys, const void *d_vals, uint64_t n, int precision, const uint64_t *d_boards,
+                     uint64_t m, int canonicalize, double *d_out)
+{
+    CGB_TRY(ensure_init());
+    if (precision != 32 && precision != 64) {
+        set_error("cgb_lookup_batch: precision must be 32 or 64");
+        return -1;
+    }
+    cudaStream_t s = E().stream;
+    LayerIndex ix;
+    ix.keys = d_keys;
+    ix.vals = d_vals;
+    ix.n = n;
+    const int vb = precision == 32 ? 4 : 8;
+    IndexStorage st;
+    const bool ok = build_index(ix, E().index_kind, vb, st, E().bucket_bits, E().ctr, s) &&
+                    lookup_batch(ix, vb, d_boards, m, canonicalize != 0, d_out, s);
+    dev_free(st.p, s);
+    CGB_TRY(ok);
+    CGB_TRY(E().sync());
+    return 0;
+}
+
 // ---------------------------------------------------------------- sweeps
 namespace {
 

@@ -147,6 +147,21 @@ def solve_layer(keys: torch.Tensor, t2: Tuple[torch.Tensor, torch.Tensor], t4: T
     return out[: keys.numel()]
 
 
+def lookup_batch(keys: torch.Tensor, vals: torch.Tensor, boards: torch.Tensor, canonicalize: bool = False) -> torch.Tensor:
+    """Values of `boards` in one solved layer (keys sorted, vals float64 or float32) through the
+    engine's index; float64, 0.0 for a board not in the layer (lookup(), src/solve.c:108-164)."""
+    _sync()
+    precision = 32 if vals.dtype == torch.float32 else 64
+    out = torch.empty(max(boards.numel(), 1), dtype=torch.float64, device=boards.device)
+
+    def p(t):
+        return _ptr(t) if t is not None and t.numel() else None
+
+    check(lib().cgb_lookup_batch(p(keys), p(vals), keys.numel(), precision, p(boards), boards.numel(),
+                                 1 if canonicalize else 0, _ptr(out)))
+    return out[: boards.numel()]
+
+
 def generate(initial: Sequence[int], start: int, end: int, keep: bool = True):
     """Generation sweep; returns ({sum: numpy layer}, stats dict)."""
     layers: Dict[int, np.ndarray] = {}

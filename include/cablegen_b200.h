@@ -115,6 +115,17 @@ int cgb_solve_layer(const uint64_t *d_keys, uint64_t n, void *d_out, int precisi
                     const void *d_v2, uint64_t n2, const uint64_t *d_k4, const void *d_v4, uint64_t n4,
                     const uint64_t *h_winstates, int n_winstates);
 
+/* ---- lookup of many boards (lookup(), src/solve.c:108-164) ---------------
+ * (d_keys, d_vals, n): one solved layer on the device, keys sorted; d_vals
+ * double (precision 64) or float (32).  The layer gets the index the solve
+ * builds (option "index"), then every board of d_boards[m] is looked up --
+ * canonicalised first when canonicalize, as lookup() does -- and its value
+ * written to d_out[m] as a double (0.0 for a board not in the layer).  For
+ * consumers that look up many positions at once; lookup() itself stays the
+ * host search over a table the caller holds. */
+int cgb_lookup_batch(const uint64_t *d_keys, const void *d_vals, uint64_t n, int precision, const uint64_t *d_boards,
+                     uint64_t m, int canonicalize, double *d_out);
+
 /* ---- whole sweeps -------------------------------------------------------- */
 typedef struct {
     uint64_t layers, boards_generated, boards_solved;
